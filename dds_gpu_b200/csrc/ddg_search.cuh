@@ -1,0 +1,534 @@
+// The exact double-dummy search of one solver lane, as a resumable stage machine.
+//
+// A search answers "can NS take >= target tricks?" (null window); the trick count of a
+// lead comes from a binary search over targets (first 7, then the previous lead's answer)
+// or, with a seed, from stepping up or down from it. This is the reference's method
+// (src/dd.h:613-939, src/dd_wave.h:1-147). Node counts equal the reference's because the
+// order of moves, the bounds that fire and the TT decisions are the same.
+//
+// What is new is the layout for a GPU lane: the position lives in registers (hands, the
+// current trick packed into one word), the frame on top of the stack too (48 bytes,
+// written to the lane's stack in HBM only when a child is entered, read back when it
+// returns), and the trick-start TT key is recomputed at the store instead of being kept
+// per level. One call of lane_step() runs one stage; a warp runs one stage at a time for
+// all lanes that are in it.
+#pragma once
+#include "ddg_order.cuh"
+#include "ddg_tt.cuh"
+
+namespace ddg {
+
+struct Pos {
+  u64 h[4];
+  u32 trick;  // cards of the current trick in play order, a byte each
+  int trump, leader, nplayed, ns_won, left;
+};
+
+// One level of the search (48 bytes; 16-byte aligned in the lane's stack).
+struct alignas(16) Frame {
+  u64 acc;    // relevant cards gathered from the children so far
+  u64 tried;  // cards tried at this node
+  u64 mv_lo;  // candidate cards 0..7, a byte each
+  u64 mv_hi;  // candidates 8..12 (bytes 0..4), count (byte 5), next index (6), cutting card (7)
+  u32 undo;   // the trick's cards when this ply completed it
+  u32 info;   // result:1 | seat:2 | need:4 | lb:4 | ub:4 | undo leader:2 | -:7 | win card:8
+  u64 pad;
+};
+static_assert(sizeof(Frame) == 48, "frame is three 16-byte words");
+
+DDG_HD int fr_byte(const Frame& f, int k) {
+  u64 w = k < 8 ? f.mv_lo : f.mv_hi;
+  return (int)((w >> (8 * (k & 7))) & 0xFF);
+}
+DDG_HD int fr_move(const Frame& f, int k) { return fr_byte(f, k); }
+DDG_HD int fr_n(const Frame& f) { return fr_byte(f, 13); }
+DDG_HD int fr_i(const Frame& f) { return fr_byte(f, 14); }
+DDG_HD int fr_best(const Frame& f) { return (int)(int8_t)(uint8_t)fr_byte(f, 15); }
+DDG_HD void fr_set_hi_byte(Frame& f, int k, int v) {
+  int sh = 8 * (k - 8);
+  f.mv_hi = (f.mv_hi & ~((u64)0xFF << sh)) | ((u64)(v & 0xFF) << sh);
+}
+DDG_HD void fr_set_i(Frame& f, int i) { fr_set_hi_byte(f, 14, i); }
+DDG_HD void fr_set_best(Frame& f, int c) { fr_set_hi_byte(f, 15, c); }
+DDG_HD int fr_result(const Frame& f) { return (int)(f.info & 1); }
+DDG_HD int fr_seat(const Frame& f) { return (int)((f.info >> 1) & 3); }
+DDG_HD int fr_need(const Frame& f) { return (int)((f.info >> 3) & 15); }
+DDG_HD int fr_lb(const Frame& f) { return (int)((f.info >> 7) & 15); }
+DDG_HD int fr_ub(const Frame& f) { return (int)((f.info >> 11) & 15); }
+DDG_HD int fr_undo_leader(const Frame& f) { return (int)((f.info >> 15) & 3); }
+DDG_HD int fr_win_card(const Frame& f) { return (int)(int8_t)(uint8_t)(f.info >> 24); }
+DDG_HD void fr_set_result(Frame& f, int v) { f.info = (f.info & ~1u) | (u32)(v & 1); }
+
+DDG_HD void frame_load(Frame& f, const Frame* p) {
+#ifdef __CUDA_ARCH__
+  const ulonglong2* v = reinterpret_cast<const ulonglong2*>(p);
+  ulonglong2 a = v[0], b = v[1], c = v[2];
+  f.acc = a.x;
+  f.tried = a.y;
+  f.mv_lo = b.x;
+  f.mv_hi = b.y;
+  f.undo = (u32)c.x;
+  f.info = (u32)(c.x >> 32);
+  f.pad = 0;
+#else
+  f = *p;
+#endif
+}
+DDG_HD void frame_store(Frame* p, const Frame& f) {
+#ifdef __CUDA_ARCH__
+  ulonglong2* v = reinterpret_cast<ulonglong2*>(p);
+  v[0] = make_ulonglong2(f.acc, f.tried);
+  v[1] = make_ulonglong2(f.mv_lo, f.mv_hi);
+  v[2] = make_ulonglong2((u64)f.undo | ((u64)f.info << 32), 0);
+#else
+  *p = f;
+#endif
+}
+
+// Search counters of one lane.
+struct LaneStats {
+  u64 nodes;
+  TTStats tt;
+  u64 enter_exit[7];  // trivial, last trick, TT hit, quick tricks, later tricks, QT 2nd hand, expanded
+};
+
+DDG_HD int trick_at(const Pos& p, int i) { return trick_card(p.trick, i); }
+
+// Trick winner's index among the first n cards.
+DDG_HD int winning_index(const Pos& p, int n) {
+  int w = 0;
+  for (int i = 1; i < n; i++)
+    if (beats(trick_at(p, i), trick_at(p, w), p.trump)) w = i;
+  return w;
+}
+
+// Candidate cards for `seat`, one per run of alike cards, best first (ties: higher card
+// index first). Writes them with their count into the frame.
+DDG_HD int gen_moves(const Pos& p, int seat, int hint, const Top& top, Frame& f) {
+  const u64 own = hand_at(p.h, seat);
+  u64 legal = own;
+  u64 all = all_cards(p.h);
+  if (p.nplayed) {
+    u64 follow = own & suit_cards(card_suit(trick_at(p, 0)));
+    if (follow) legal = follow;
+    for (int i = 0; i < p.nplayed; i++) all |= card_bit(trick_at(p, i));
+  }
+  Follow fo;
+  if (p.nplayed) follow_init(fo, p.h, p.trump, p.leader, p.trick, p.nplayed);
+  u64 rest = legal & run_tops(own, all);
+  int n = 0;
+  int score[13];
+  int card_of[13];
+  while (rest) {
+    int card = top_bit(rest);
+    rest ^= card_bit(card);
+    bool hinted = hint >= 0 && alike(own, all, hint, card);
+    int sc = p.nplayed == 0 ? lead_weight(p.h, top, p.trump, p.left, seat, card, hinted)
+                            : (hinted ? 1000 : follow_weight(fo, p.h, p.trump, p.nplayed, seat, card));
+    int i = n++;
+    while (i > 0 && score[i - 1] < sc) {
+      score[i] = score[i - 1];
+      card_of[i] = card_of[i - 1];
+      i--;
+    }
+    score[i] = sc;
+    card_of[i] = card;
+  }
+  u64 lo = 0, hi = 0;
+  for (int k = 0; k < n; k++) {
+    if (k < 8) lo |= (u64)card_of[k] << (8 * k);
+    else hi |= (u64)card_of[k] << (8 * (k - 8));
+  }
+  f.mv_lo = lo;
+  f.mv_hi = hi | (u64)n << 40 | (u64)0xFF << 56;  // next index 0, no cutting card yet
+  return n;
+}
+
+// Enters the node at the current position (src/dd.h:626-737). Returns 0/1 when decided at
+// once (`rel` set), else -1 with `f` holding the ordered candidates.
+DDG_HD int enter(Pos& p, int target, Frame& f, u64& rel, TTBucket* tt, u32 mask, u32 gen,
+                 LaneStats& st) {
+  st.nodes++;
+  int need = 0, hint = -1, ub = 0;
+  Top top;
+  if (p.nplayed == 0) {
+    rel = 0;
+    if (p.ns_won >= target) {
+      st.enter_exit[0]++;
+      return 1;
+    }
+    if (p.ns_won + p.left < target) {
+      st.enter_exit[0]++;
+      return 0;
+    }
+    need = target - p.ns_won;
+    const u64 all = all_cards(p.h);
+    if (p.left == 1) {
+      // Last trick: the highest trump, else the highest card of the suit led.
+      int s = (p.trump >= 0 && (all & suit_cards(p.trump))) ? p.trump
+                                                            : card_suit(top_bit(hand_at(p.h, p.leader)));
+      u64 in = all & suit_cards(s);
+      int hi = top_bit(in);
+      if (popc(in) >= 2) rel = card_bit(hi);
+      st.enter_exit[1]++;
+      return ns_side(holder_of(p.h, hi)) ? 1 : 0;
+    }
+    NodeKey key;
+    make_key(key, p.h, p.leader, p.left, gen, mask);
+    int hit = tt_probe(tt, key, need, rel, hint, st.tt);
+    if (hit >= 0) {
+      st.enter_exit[2]++;
+      return hit;
+    }
+    ub = p.left;
+    top_init(top, p.h, key.lens);
+    const bool ns_lead = ns_side(p.leader);
+    const int cut_ns = need, cut_ew = p.left - need + 1;
+    u64 wr = 0;
+    bool decided;
+    int q = quick_tricks(p.h, top, p.trump, p.leader, ns_lead ? cut_ns : cut_ew,
+                         ns_lead ? cut_ew : cut_ns, wr, decided);
+    if (decided) {
+      bool val = ns_lead ? q != 0 : q == 0;
+      tt_store(tt, key, gen, wr, val ? need : 0, val ? p.left : need - 1, -1, st.tt);
+      rel = wr;
+      st.enter_exit[3]++;
+      return val ? 1 : 0;
+    }
+    wr = 0;
+    bool lt = ns_lead ? !later_min(top, p.trump, p.leader, p.ns_won, p.left, target, wr)
+                      : later_max(top, p.trump, p.leader, p.ns_won, p.left, target, wr);
+    if (lt) {
+      bool val = !ns_lead;
+      tt_store(tt, key, gen, wr, val ? need : 0, val ? p.left : need - 1, -1, st.tt);
+      rel = wr;
+      st.enter_exit[4]++;
+      return val ? 1 : 0;
+    }
+  } else if (p.nplayed == 1) {
+    // Second hand: the trick-start table, with the led card given back to the leader.
+    u64 th[4] = {p.h[0], p.h[1], p.h[2], p.h[3]};
+    toggle_card(th, p.leader, trick_at(p, 0));
+    top_init(top, th, length_key(th));
+    int second = lho_of(p.leader);
+    int need2 = target - p.ns_won;
+    int cutoff = ns_side(second) ? need2 : p.left - need2 + 1;
+    u64 wr;
+    if (quick_tricks_2nd(p.h, top, p.trump, second, trick_at(p, 0), cutoff, wr)) {
+      rel = wr;
+      st.enter_exit[5]++;
+      return ns_side(second) ? 1 : 0;
+    }
+  }
+  const int seat = (p.leader + p.nplayed) & 3;
+  gen_moves(p, seat, hint, top, f);
+  f.acc = 0;
+  f.tried = 0;
+  f.undo = 0;
+  f.pad = 0;
+  // result starts as the value when no child cuts: NS to play fails, EW to play holds.
+  f.info = (u32)(!ns_side(seat)) | (u32)seat << 1 | (u32)need << 3 | (u32)0 << 7 | (u32)ub << 11 |
+           0xFFu << 24;
+  st.enter_exit[6]++;
+  return -1;
+}
+
+// Plays the frame's card (src/dd.h:739-756); at the fourth card the trick is settled and
+// the frame keeps what unplay needs.
+DDG_HD void play(Pos& p, Frame& f, int card) {
+  const int seat = fr_seat(f);
+  toggle_card(p.h, seat, card);
+  p.trick = (p.trick & ~(0xFFu << (8 * p.nplayed))) | ((u32)card << (8 * p.nplayed));
+  p.nplayed++;
+  if (p.nplayed == 4) {
+    int wi = winning_index(p, 4);
+    int w = (p.leader + wi) & 3;
+    int wc = trick_at(p, wi), same = 0;
+    for (int k = 0; k < 4; k++) same += card_suit(trick_at(p, k)) == card_suit(wc);
+    f.undo = p.trick;
+    f.info = (f.info & ~(3u << 15) & ~(0xFFu << 24)) | ((u32)p.leader << 15) |
+             ((u32)(same >= 2 ? wc : 0xFF) << 24);  // won by rank: the card is relevant
+    p.leader = w;
+    p.nplayed = 0;
+    p.left--;
+    p.ns_won += ns_side(w);
+  }
+}
+
+DDG_HD void unplay(Pos& p, const Frame& f, int card, u64& rel) {
+  if (p.nplayed == 0) {  // this ply completed a trick
+    p.trick = f.undo;
+    p.ns_won -= ns_side(p.leader);
+    p.left++;
+    p.nplayed = 4;
+    p.leader = fr_undo_leader(f);
+    int wc = fr_win_card(f);
+    if (wc >= 0) rel |= card_bit(wc);
+  }
+  p.nplayed--;
+  toggle_card(p.h, fr_seat(f), card);
+}
+
+// All moves of `f` are done (src/dd.h:772-797): widen the relevant cards through runs of
+// the hand's own touching cards, and store trick-start results in the TT.
+DDG_HD u64 finish(const Pos& p, const Frame& f, TTBucket* tt, u32 mask, u32 gen, LaneStats& st) {
+  u64 acc = f.acc;
+  const u64 own = hand_at(p.h, fr_seat(f));
+  u64 all = all_cards(p.h);
+  for (int i = 0; i < p.nplayed; i++) all |= card_bit(trick_at(p, i));
+  for (int s = 0; s < 4; s++) {
+    u64 r = acc & suit_cards(s);
+    if (!r) continue;
+    int low = low_bit(r);
+    while ((own >> low) & 1) {
+      u64 below = all & suit_cards(s) & (card_bit(low) - 1);
+      if (!below || !((own >> top_bit(below)) & 1)) break;
+      low = top_bit(below);
+      acc |= card_bit(low);
+    }
+  }
+  if (p.nplayed == 0) {
+    int lb = fr_lb(f), ub = fr_ub(f);
+    if (fr_result(f)) lb = fr_need(f);
+    else ub = fr_need(f) - 1;
+    NodeKey key;
+    make_key(key, p.h, p.leader, p.left, gen, mask);
+    tt_store(tt, key, gen, acc, lb, ub, fr_best(f), st.tt);
+  }
+  return acc;
+}
+
+// ---- the stage machine ------------------------------------------------------------------
+
+enum Stage { ST_TAKE = 0, ST_ROOT = 1, ST_ENTER = 2, ST_NEXT = 3, ST_RET = 4, ST_IDLE = 5, ST_COUNT = 6 };
+
+// How a lead's trick count is found.
+enum { MODE_BISECT = 0, MODE_STEP = 1 };
+// Phases of MODE_STEP: first search at the seed, stepping up, stepping down.
+enum { PH_FIRST = 0, PH_UP = 1, PH_DOWN = 2 };
+
+struct Lane {
+  Pos p;
+  Frame f;        // top of the stack
+  int stage, sp;  // sp = depth of f; frames 0..sp-1 are in the lane's stack
+  int target;     // the null-window search in progress: NS >= target?
+  int lo, hi;     // MODE_BISECT: answer in [lo, hi]; MODE_STEP: lo = t, hi = phase
+  int mode, decl, last_decl, strain;
+  long long job, deal;
+  int v;   // value of the node just finished
+  u64 r;   // its relevant cards
+  u32 gen;
+  LaneStats st;
+};
+
+// Sets up the search of declarer `decl`'s lead (leader = decl + 1) at `target`.
+DDG_HD void start_search(Lane& L) {
+  L.p.leader = (L.decl + 1) & 3;
+  L.p.nplayed = 0;
+  L.p.ns_won = 0;
+  L.p.left = popc(L.p.h[0]);
+  L.p.trick = 0;
+  L.sp = 0;
+  L.stage = ST_ENTER;
+}
+
+// Starts the trick count of the current declarer: the binary search at `first`, or the
+// stepping search from the seed `first`.
+DDG_HD void start_lead(Lane& L, int first) {
+  if (L.mode == MODE_BISECT) {
+    L.lo = 0;
+    L.hi = 13;
+    L.target = first < 1 ? 1 : first > 13 ? 13 : first;
+    start_search(L);
+    return;
+  }
+  int left = popc(L.p.h[0]);
+  int t = first < 0 ? 0 : first > left ? left : first;
+  L.lo = t;
+  if (t == 0) {  // ">= 0" needs no search
+    L.hi = PH_UP;
+    L.target = 1;
+  } else {
+    L.hi = PH_FIRST;
+    L.target = t;
+  }
+  if (L.hi == PH_UP && L.lo >= left) {
+    L.target = -1;  // answer known: lo
+    return;
+  }
+  start_search(L);
+}
+
+// A root search finished with L.v: next target, or the lead's answer (>= 0) when known.
+DDG_HD int root_result(Lane& L) {
+  if (L.mode == MODE_BISECT) {
+    if (L.v) L.lo = L.target;
+    else L.hi = L.target - 1;
+    if (L.lo < L.hi) {
+      L.target = (L.lo + L.hi + 1) / 2;
+      return -1;
+    }
+    return L.lo;
+  }
+  int left = popc(L.p.h[0]);
+  int t = L.lo;
+  if (L.hi == PH_FIRST || L.hi == PH_UP) {
+    if (L.hi == PH_FIRST && !L.v) {
+      t--;
+      L.lo = t;
+      L.hi = PH_DOWN;
+      if (t <= 0) return 0;
+      L.target = t;
+      return -1;
+    }
+    if (L.hi == PH_UP) {
+      if (!L.v) return t;
+      t++;
+    }
+    L.lo = t;
+    L.hi = PH_UP;
+    if (t >= left) return t;
+    L.target = t + 1;
+    return -1;
+  }
+  // PH_DOWN: searching t
+  if (L.v) return t;
+  t--;
+  L.lo = t;
+  if (t <= 0) return 0;
+  L.target = t;
+  return -1;
+}
+
+// The environment a lane runs in (a GPU block, or the host replay in the tests):
+//   bool take(Lane&)            next job: fills deal, strain, decl, last_decl, mode, hands;
+//                               false when there is none
+//   int seed(const Lane&)       first target / seed of the current declarer
+//   void answer(const Lane&, int tricks)  result of the current declarer
+//   void job_done(const Lane&)  the lane's job is finished
+//   Frame* stack                the lane's frames (depth 0..52)
+//   TTBucket* tt; u32 mask      the lane's TT
+template <class Env>
+DDG_HD void node_done(Lane& L, Env& env) {
+  if (L.sp > 0) {
+    L.sp--;
+    frame_load(L.f, env.stack + L.sp);
+    L.stage = ST_RET;
+    return;
+  }
+  int ans = root_result(L);
+  if (ans < 0) {
+    start_search(L);
+    return;
+  }
+  for (;;) {
+    env.answer(L, ans);
+    L.decl++;
+    if (L.decl > L.last_decl) {
+      env.job_done(L);
+      L.stage = ST_TAKE;
+      return;
+    }
+    // The next lead starts at this answer (binary search) or at its own seed.
+    start_lead(L, L.mode == MODE_BISECT ? ans : env.seed(L));
+    if (L.target >= 0) return;
+    ans = L.lo;
+  }
+}
+
+template <class Env>
+DDG_HD void lane_step(Lane& L, Env& env) {
+  switch (L.stage) {
+    case ST_TAKE: {
+      if (!env.take(L)) {
+        L.stage = ST_IDLE;
+        return;
+      }
+      L.p.trump = strain_trump(L.strain);
+      L.p.trick = 0;
+      L.gen = tt_next_gen(env.tt, env.mask, L.gen);
+      L.stage = ST_ROOT;
+      return;
+    }
+    case ST_ROOT: {
+      start_lead(L, env.seed(L));
+      if (L.target < 0) {  // answered without a search
+        L.sp = 0;
+        L.v = 1;
+        int ans = L.lo;
+        for (;;) {
+          env.answer(L, ans);
+          L.decl++;
+          if (L.decl > L.last_decl) {
+            env.job_done(L);
+            L.stage = ST_TAKE;
+            return;
+          }
+          start_lead(L, L.mode == MODE_BISECT ? ans : env.seed(L));
+          if (L.target >= 0) return;
+          ans = L.lo;
+        }
+      }
+      return;
+    }
+    case ST_ENTER: {
+      int e = enter(L.p, L.target, L.f, L.r, env.tt, env.mask, L.gen, L.st);
+      if (e < 0) {
+        L.stage = ST_NEXT;
+        return;
+      }
+      L.v = e;
+      node_done(L, env);
+      return;
+    }
+    case ST_NEXT: {
+      Frame& f = L.f;
+      int i = fr_i(f);
+      const int n = fr_n(f);
+      while (i < n) {
+        int card = fr_move(f, i);
+        int s = card_suit(card);
+        // Cards below every relevant card of their suit are alike: one of them is tried.
+        u64 rs = f.acc & suit_cards(s);
+        u64 small = rs ? (card_bit(low_bit(rs)) - 1) & suit_cards(s) : suit_cards(s);
+        if ((small & card_bit(card)) && (small & f.tried)) {
+          i++;
+          continue;
+        }
+        fr_set_i(f, i);
+        f.tried |= card_bit(card);
+        play(L.p, f, card);
+        frame_store(env.stack + L.sp, f);
+        L.sp++;
+        L.stage = ST_ENTER;
+        return;
+      }
+      fr_set_i(f, i);
+      L.v = fr_result(f);
+      L.r = finish(L.p, f, env.tt, env.mask, L.gen, L.st);
+      node_done(L, env);
+      return;
+    }
+    case ST_RET: {
+      Frame& f = L.f;
+      int card = fr_move(f, fr_i(f));
+      unplay(L.p, f, card, L.r);
+      if (L.v == (int)ns_side(fr_seat(f))) {  // the child cuts
+        fr_set_result(f, L.v);
+        f.acc = L.r;
+        fr_set_best(f, card);
+        L.r = finish(L.p, f, env.tt, env.mask, L.gen, L.st);
+        node_done(L, env);
+        return;
+      }
+      f.acc |= L.r;
+      fr_set_i(f, fr_i(f) + 1);
+      L.stage = ST_NEXT;
+      return;
+    }
+    default:
+      return;
+  }
+}
+
+}  // namespace ddg

@@ -1,0 +1,262 @@
+// Exact partition-search transposition table, one per solver lane.
+//
+// Layout (per lane: 2^tt_log2 buckets of 320 bytes, 64-byte aligned):
+//   tag[16]   one 64-byte line, read by a probe as four 128-bit loads
+//   e[16]     16-byte entries (w0, w1)
+// A tag is hash bits 48..63 (16) | tricks left (4) | way of its entry (4) | generation (6) |
+// leader (2), 0 = empty; tags stay in age order (newest first) while entries stay in
+// place, so a store rewrites one tag line and one entry. The entry packing
+//   w0: q = hash bits 9..47 (39) | lb (4) | ub (4) | best card (6, 63 none) | owners 48..57
+//   w1: relevant-card counts per suit (4 bits each) | owners 0..47
+// and the eviction rule (least 2*left + age, other generations first) are the
+// reference's (src/dd.h:87-111, 325-350, 438-532): both decide which positions the TT
+// answers and so the node counts, which the tests compare one for one.
+#pragma once
+#include "ddg_bits.cuh"
+
+namespace ddg {
+
+enum { TT_WAYS = 16, GEN_BITS = 6, Q_BITS = 39, MAX_REL = 29, TT_MIN_LOG2 = 9 };
+
+struct alignas(64) TTBucket {
+  u32 tag[TT_WAYS];
+  u64 e[TT_WAYS][2];
+};
+static_assert(sizeof(TTBucket) == 320, "bucket is 5 x 64 bytes");
+
+// Trick-start key of a position: what the TT needs to look it up and to store it.
+struct NodeKey {
+  u64 code[4];  // suit_codes()
+  u64 all;      // cards in play
+  u64 lens;     // length_key()
+  u64 q;        // hash bits 9..47
+  u32 bucket;   // hash bits 0..tt_log2-1
+  u32 tag;      // tag without its way
+};
+
+DDG_HD void make_key(NodeKey& k, const u64* h, int leader, int left, u32 gen, u32 mask) {
+  suit_codes(h, k.code);
+  k.all = all_cards(h);
+  k.lens = length_key(h);
+  u64 x = key_hash(k.lens, leader);
+  k.bucket = (u32)x & mask;
+  k.q = (x >> 9) & ((1ull << Q_BITS) - 1);
+  k.tag = ((u32)(x >> 32) & 0xFFFF0000u) | ((u32)left << 12) | (gen << 2) | (u32)leader;
+}
+
+// Traffic counters of the TT, in bytes (what the roofline counts as algorithmic bytes).
+struct TTStats {
+  u64 probes, hits, stores, rd_bytes, wr_bytes;
+};
+
+DDG_HD void tags_load(const TTBucket* b, u32* t) {
+#ifdef __CUDA_ARCH__
+  const uint4* v = reinterpret_cast<const uint4*>(b->tag);
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    uint4 x = v[k];
+    t[4 * k] = x.x;
+    t[4 * k + 1] = x.y;
+    t[4 * k + 2] = x.z;
+    t[4 * k + 3] = x.w;
+  }
+#else
+  for (int k = 0; k < TT_WAYS; k++) t[k] = b->tag[k];
+#endif
+}
+DDG_HD void tags_store(TTBucket* b, const u32* t) {
+#ifdef __CUDA_ARCH__
+  uint4* v = reinterpret_cast<uint4*>(b->tag);
+#pragma unroll
+  for (int k = 0; k < 4; k++) v[k] = make_uint4(t[4 * k], t[4 * k + 1], t[4 * k + 2], t[4 * k + 3]);
+#else
+  for (int k = 0; k < TT_WAYS; k++) b->tag[k] = t[k];
+#endif
+}
+DDG_HD void entry_load(const TTBucket* b, int way, u64& w0, u64& w1) {
+#ifdef __CUDA_ARCH__
+  ulonglong2 x = *reinterpret_cast<const ulonglong2*>(b->e[way]);
+  w0 = x.x;
+  w1 = x.y;
+#else
+  w0 = b->e[way][0];
+  w1 = b->e[way][1];
+#endif
+}
+DDG_HD void entry_store(TTBucket* b, int way, u64 w0, u64 w1) {
+#ifdef __CUDA_ARCH__
+  *reinterpret_cast<ulonglong2*>(b->e[way]) = make_ulonglong2(w0, w1);
+#else
+  b->e[way][0] = w0;
+  b->e[way][1] = w1;
+#endif
+}
+
+// Positions (bit k) whose tag equals `tag` apart from the way, and the ways of all 16
+// tags packed 4 bits each.
+DDG_HD u32 tag_matches(const u32* t, u32 tag, u64& ways) {
+  u32 m = 0;
+  ways = 0;
+#pragma unroll
+  for (int k = 0; k < TT_WAYS; k++) {
+    m |= (u32)((t[k] & ~0xF00u) == tag) << k;
+    ways |= (u64)((t[k] >> 8) & 15) << (4 * k);
+  }
+  return m;
+}
+
+// Looks up bounds of the NS tricks still to win. Returns 1 (NS reach `need`), 0 (they do
+// not), or -1 (unknown; `hint` = the stored best move of a matching entry, if any).
+DDG_HD int tt_probe(const TTBucket* tt, const NodeKey& k, int need, u64& rel, int& hint,
+                    TTStats& st) {
+  const TTBucket* b = tt + k.bucket;
+  u32 t[TT_WAYS];
+  tags_load(b, t);
+  u64 ways;
+  u32 m = tag_matches(t, k.tag, ways);
+  st.probes++;
+  st.rd_bytes += 64;
+  int lens_s[4];
+#pragma unroll
+  for (int s = 0; s < 4; s++) lens_s[s] = code_len(k.code[s]);
+  while (m) {
+    int pos = low_bit32(m);
+    m &= m - 1;
+    u64 w0, w1;
+    entry_load(b, (int)((ways >> (4 * pos)) & 15), w0, w1);
+    st.rd_bytes += 16;
+    if ((w0 & ((1ull << Q_BITS) - 1)) != k.q) continue;
+    u64 owners = (w1 >> 16) | ((w0 >> 53) << 48);
+    int off = 0;
+    bool same = true;
+    int cnt[4];
+#pragma unroll
+    for (int s = 0; s < 4; s++) {
+      int n = (int)((w1 >> (4 * s)) & 15);
+      cnt[s] = n;
+      if (n > lens_s[s]) {
+        same = false;
+      } else {
+        u64 stored = ((owners >> off) & ((1ull << (2 * n)) - 1)) | (1ull << (2 * n));
+        same = same && (k.code[s] >> (2 * (lens_s[s] - n))) == stored;
+      }
+      off += 2 * n;
+    }
+    if (!same) continue;
+    int lb = (int)((w0 >> Q_BITS) & 15), ub = (int)((w0 >> (Q_BITS + 4)) & 15);
+    if (lb >= need || ub < need) {
+      u64 r = 0;
+#pragma unroll
+      for (int s = 0; s < 4; s++) r |= top_n_cards(k.all, s, cnt[s]);
+      rel = r;
+      st.hits++;
+      return lb >= need ? 1 : 0;
+    }
+    int bm = (int)((w0 >> (Q_BITS + 8)) & 63);
+    if (bm != 63) hint = bm;
+  }
+  return -1;
+}
+
+// Owner patterns of the relevant cards for w1 and w0's top bits; false when more than
+// MAX_REL cards are relevant (such results are not stored).
+DDG_HD bool pack_owners(const NodeKey& k, u64 rel, u64& w1, u64& hi) {
+  u64 counts = 0, owners = 0;
+  int total = 0;
+#pragma unroll
+  for (int s = 0; s < 4; s++) {
+    u64 p = rel_pattern(k.code[s], k.all, rel, s);
+    int n = code_len(p);
+    if (total + n > MAX_REL) return false;
+    counts |= (u64)n << (4 * s);
+    owners |= (p ^ (1ull << (2 * n))) << (2 * total);
+    total += n;
+  }
+  w1 = counts | (owners << 16);
+  hi = (owners >> 48) << 53;
+  return true;
+}
+
+DDG_HD u64 pack_w0(const NodeKey& k, int lb, int ub, int best, u64 hi) {
+  return k.q | (u64)lb << Q_BITS | (u64)ub << (Q_BITS + 4) | (u64)(best < 0 ? 63 : best) << (Q_BITS + 8) | hi;
+}
+
+// Stores bounds [lb, ub] of the NS tricks still to win for the class of positions that
+// share `rel`'s relevant cards with this one. An entry with the same key is narrowed in
+// place; otherwise a way is taken (empty, else other generation, else least
+// 2 * tricks left + age) and its tag put in front.
+DDG_HD void tt_store(TTBucket* tt, const NodeKey& k, u32 gen, u64 rel, int lb, int ub, int best,
+                     TTStats& st) {
+  u64 w1, hi;
+  if (!pack_owners(k, rel, w1, hi)) return;
+  TTBucket* b = tt + k.bucket;
+  u32 t[TT_WAYS];
+  tags_load(b, t);
+  st.rd_bytes += 64;
+  st.stores++;
+  u64 ways;
+  u32 m = tag_matches(t, k.tag, ways);
+  while (m) {
+    int pos = low_bit32(m);
+    m &= m - 1;
+    int way = (int)((ways >> (4 * pos)) & 15);
+    u64 e0, e1;
+    entry_load(b, way, e0, e1);
+    st.rd_bytes += 16;
+    if ((e0 & ((1ull << Q_BITS) - 1)) == k.q && e1 == w1 && (e0 >> 53 << 53) == hi) {
+      int olb = (int)((e0 >> Q_BITS) & 15), oub = (int)((e0 >> (Q_BITS + 4)) & 15);
+      int obest = (int)((e0 >> (Q_BITS + 8)) & 63);
+      if (olb > lb) lb = olb;
+      if (oub < ub) ub = oub;
+      if (best < 0 && obest != 63) best = obest;
+#ifdef __CUDA_ARCH__
+      reinterpret_cast<u64*>(b->e[way])[0] = pack_w0(k, lb, ub, best, hi);
+#else
+      b->e[way][0] = pack_w0(k, lb, ub, best, hi);
+#endif
+      st.wr_bytes += 8;
+      return;
+    }
+  }
+  // Take a way: position `pos` leaves the line, the tags in front of it move back one.
+  int pos = TT_WAYS - 1, way;
+  if (t[TT_WAYS - 1] != 0) {
+    int least = 99;
+#pragma unroll
+    for (int p = TT_WAYS - 1; p >= 0; p--) {
+      int v = ((t[p] >> 2) & 63) != gen ? -1 : 2 * (int)((t[p] >> 12) & 15) + TT_WAYS - 1 - p;
+      if (v < least) {
+        least = v;
+        pos = p;
+      }
+    }
+    way = (int)((ways >> (4 * pos)) & 15);
+  } else {
+    u32 empty = 0;  // while the line is not full its used tags are positions 0..n-1
+#pragma unroll
+    for (int p = 0; p < TT_WAYS; p++) empty |= (u32)(t[p] == 0) << p;
+    way = low_bit32(empty);
+  }
+#pragma unroll
+  for (int i = TT_WAYS - 1; i > 0; i--)
+    if (i <= pos) t[i] = t[i - 1];
+  t[0] = k.tag | ((u32)way << 8);
+  tags_store(b, t);
+  entry_store(b, way, pack_w0(k, lb, ub, best, hi), w1);
+  st.wr_bytes += 64 + 16;
+}
+
+// Next generation of a lane's TT; at the wrap all tags are cleared.
+DDG_HD u32 tt_next_gen(TTBucket* tt, u32 mask, u32 gen) {
+  gen++;
+  if (gen >= (1u << GEN_BITS)) {
+    u32 zero[TT_WAYS];
+#pragma unroll
+    for (int k = 0; k < TT_WAYS; k++) zero[k] = 0;
+    for (u32 i = 0; i <= mask; i++) tags_store(tt + i, zero);
+    gen = 1;
+  }
+  return gen;
+}
+
+}  // namespace ddg
