@@ -1,0 +1,169 @@
+"""B200-native exact double-dummy solver.
+
+A ctypes binding of the C ABI in ``include/ddg.h`` (``_lib/libddg.so``, built by
+``python -m dds_gpu_b200.build``). The library runs the search only on the GPU: there is no
+CPU fallback, and a missing library or device is an error.
+
+Card model (the reference's, src/dd.h:13-14): hand = uint64 with bit suit*16+rank, suits
+S,H,D,C, ranks 2..A = 0..12; seats N,E,S,W; strains C,D,H,S,NT. Results are
+``tricks[deal, strain, declarer]`` (uint8; 255 = not solved).
+"""
+import ctypes
+import os
+
+import numpy as np
+
+__all__ = ["Solver", "DDGError", "make_deals", "check_deal", "library_path", "load_library"]
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_lib", "libddg.so")
+_lib = None
+
+
+class DDGError(RuntimeError):
+    """A libddg call failed; the message is ddg_last_error()."""
+
+
+class _Config(ctypes.Structure):
+    _fields_ = [("tt_log2", ctypes.c_int), ("lanes", ctypes.c_int), ("block", ctypes.c_int),
+                ("jobs_per_deal", ctypes.c_int), ("device", ctypes.c_int), ("schedule", ctypes.c_int),
+                ("time_limit_s", ctypes.c_double), ("mem_fraction", ctypes.c_double)]
+
+
+class _Stats(ctypes.Structure):
+    _fields_ = [("nodes", ctypes.c_uint64), ("tt_probes", ctypes.c_uint64), ("tt_hits", ctypes.c_uint64),
+                ("tt_stores", ctypes.c_uint64), ("tt_bytes", ctypes.c_uint64),
+                ("enter_exit", ctypes.c_uint64 * 7), ("stage_iters", ctypes.c_uint64 * 6),
+                ("stage_lanes", ctypes.c_uint64 * 6), ("jobs_done", ctypes.c_int64),
+                ("kernel_ms", ctypes.c_double), ("lanes", ctypes.c_int), ("grid", ctypes.c_int),
+                ("block", ctypes.c_int)]
+
+    def as_dict(self):
+        d = {}
+        for name, _ in self._fields_:
+            v = getattr(self, name)
+            d[name] = list(v) if isinstance(v, ctypes.Array) else v
+        return d
+
+
+P = ctypes.c_void_p
+
+
+def library_path():
+    return _LIB_PATH
+
+
+def load_library():
+    """Loads libddg.so (once). Raises DDGError when it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(_LIB_PATH):
+        raise DDGError(f"{_LIB_PATH} is missing: build it with `python -m dds_gpu_b200.build`")
+    lib = ctypes.CDLL(_LIB_PATH)
+    lib.ddg_version.restype = ctypes.c_char_p
+    lib.ddg_last_error.restype = ctypes.c_char_p
+    lib.ddg_config_default.argtypes = [ctypes.POINTER(_Config)]
+    lib.ddg_solver_create.argtypes = [ctypes.POINTER(_Config), ctypes.POINTER(P)]
+    lib.ddg_solver_destroy.argtypes = [P]
+    lib.ddg_solver_lanes.argtypes = [P]
+    lib.ddg_solver_bytes.argtypes = [P]
+    lib.ddg_solver_bytes.restype = ctypes.c_int64
+    lib.ddg_solve_batch.argtypes = [P, P, ctypes.c_int64, P, ctypes.POINTER(_Stats)]
+    lib.ddg_solve_batch_seeded.argtypes = [P, P, ctypes.c_int64, P, P, ctypes.POINTER(_Stats)]
+    lib.ddg_solve_device.argtypes = [P, P, ctypes.c_int64, P, P, P, P, ctypes.POINTER(_Stats)]
+    lib.ddg_solve_strain.argtypes = [P, P, ctypes.c_int, P, P]
+    lib.ddg_check_deal.argtypes = [P]
+    lib.ddg_make_deals.argtypes = [ctypes.c_uint64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int, P]
+    lib.ddg_make_deals.restype = None
+    _lib = lib
+    return lib
+
+
+def _check(rc):
+    if rc != 0:
+        raise DDGError(f"ddg error {rc}: {load_library().ddg_last_error().decode()}")
+
+
+def make_deals(seed, first, n, k=13):
+    """Seeded deals [first, first+n) with k cards per hand: (n, 4) uint64 (ddg_make_deals)."""
+    out = np.zeros((n, 4), dtype=np.uint64)
+    if n:
+        load_library().ddg_make_deals(ctypes.c_uint64(seed), first, n, k, out.ctypes.data)
+    return out
+
+
+def check_deal(hands4):
+    h = np.ascontiguousarray(hands4, dtype=np.uint64)
+    return load_library().ddg_check_deal(h.ctypes.data) == 0
+
+
+class Solver:
+    """A solver pool on one GPU (ddg_solver_create): per-lane TTs and stacks in HBM."""
+
+    def __init__(self, tt_log2=10, lanes=0, block=128, jobs_per_deal=5, device=0, schedule=0,
+                 time_limit_s=0.0, mem_fraction=0.85):
+        lib = load_library()
+        cfg = _Config()
+        lib.ddg_config_default(ctypes.byref(cfg))
+        cfg.tt_log2, cfg.lanes, cfg.block = tt_log2, lanes, block
+        cfg.jobs_per_deal, cfg.device, cfg.schedule = jobs_per_deal, device, schedule
+        cfg.time_limit_s, cfg.mem_fraction = time_limit_s, mem_fraction
+        self._lib = lib
+        self._h = P()
+        _check(lib.ddg_solver_create(ctypes.byref(cfg), ctypes.byref(self._h)))
+        self.config = {name: getattr(cfg, name) for name, _ in cfg._fields_}
+        self.jobs_per_deal = jobs_per_deal
+        self.last_stats = None
+
+    @property
+    def lanes(self):
+        return self._lib.ddg_solver_lanes(self._h)
+
+    @property
+    def nbytes(self):
+        return self._lib.ddg_solver_bytes(self._h)
+
+    def close(self):
+        if self._h:
+            self._lib.ddg_solver_destroy(self._h)
+            self._h = P()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def solve(self, hands, seeds=None):
+        """Tricks (n, 5, 4) uint8 for deals (n, 4) uint64 in host memory; `seeds`: optional
+        NS-trick seeds (n, 5, 4) for the stepping search."""
+        h = np.ascontiguousarray(hands, dtype=np.uint64).reshape(-1, 4)
+        n = h.shape[0]
+        out = np.empty((n, 5, 4), dtype=np.uint8)
+        st = _Stats()
+        if seeds is None:
+            _check(self._lib.ddg_solve_batch(self._h, h.ctypes.data, n, out.ctypes.data, ctypes.byref(st)))
+        else:
+            sd = np.ascontiguousarray(seeds, dtype=np.int8).reshape(n, 20)
+            _check(self._lib.ddg_solve_batch_seeded(self._h, h.ctypes.data, n, sd.ctypes.data,
+                                                    out.ctypes.data, ctypes.byref(st)))
+        self.last_stats = st.as_dict()
+        return out
+
+    def solve_device(self, d_hands, n, d_out, d_seeds=0, d_job_nodes=0, stream=0):
+        """Device-pointer form (ddg_solve_device): integer addresses of device buffers."""
+        st = _Stats()
+        _check(self._lib.ddg_solve_device(self._h, P(d_hands), n, P(d_seeds or None), P(d_out),
+                                          P(d_job_nodes or None), P(stream or None), ctypes.byref(st)))
+        self.last_stats = st.as_dict()
+        return self.last_stats
+
+    def solve_strain(self, hands4, strain, ns4=None):
+        """One strain of one deal, declarers N,E,S,W (the reference's dd_solve_strain)."""
+        h = np.ascontiguousarray(hands4, dtype=np.uint64).reshape(4)
+        out = np.zeros(4, dtype=np.int32)
+        s4 = None if ns4 is None else np.ascontiguousarray(ns4, dtype=np.int32)
+        _check(self._lib.ddg_solve_strain(self._h, h.ctypes.data, strain,
+                                          None if s4 is None else s4.ctypes.data, out.ctypes.data))
+        return [int(x) for x in out]

@@ -318,7 +318,6 @@ struct Lane {
   int v;   // value of the node just finished
   u64 r;   // its relevant cards
   u32 gen;
-  LaneStats st;
 };
 
 // Sets up the search of declarer `decl`'s lead (leader = decl + 1) at `target`.
@@ -408,6 +407,7 @@ DDG_HD int root_result(Lane& L) {
 //   void job_done(const Lane&)  the lane's job is finished
 //   Frame* stack                the lane's frames (depth 0..52)
 //   TTBucket* tt; u32 mask      the lane's TT
+//   LaneStats& stats()          the lane's counters (kept out of registers on the GPU)
 template <class Env>
 DDG_HD void node_done(Lane& L, Env& env) {
   if (L.sp > 0) {
@@ -472,7 +472,7 @@ DDG_HD void lane_step(Lane& L, Env& env) {
       return;
     }
     case ST_ENTER: {
-      int e = enter(L.p, L.target, L.f, L.r, env.tt, env.mask, L.gen, L.st);
+      int e = enter(L.p, L.target, L.f, L.r, env.tt, env.mask, L.gen, env.stats());
       if (e < 0) {
         L.stage = ST_NEXT;
         return;
@@ -505,7 +505,7 @@ DDG_HD void lane_step(Lane& L, Env& env) {
       }
       fr_set_i(f, i);
       L.v = fr_result(f);
-      L.r = finish(L.p, f, env.tt, env.mask, L.gen, L.st);
+      L.r = finish(L.p, f, env.tt, env.mask, L.gen, env.stats());
       node_done(L, env);
       return;
     }
@@ -517,7 +517,7 @@ DDG_HD void lane_step(Lane& L, Env& env) {
         fr_set_result(f, L.v);
         f.acc = L.r;
         fr_set_best(f, card);
-        L.r = finish(L.p, f, env.tt, env.mask, L.gen, L.st);
+        L.r = finish(L.p, f, env.tt, env.mask, L.gen, env.stats());
         node_done(L, env);
         return;
       }

@@ -1,0 +1,116 @@
+/* ddg.h - C ABI of the B200 double-dummy solver (libddg.so).
+ *
+ * Card model (the reference's, src/dd.h:13-14): a hand is a uint64 with bit suit*16+rank,
+ * suits 0..3 = S,H,D,C, ranks 0..12 = 2..A; seats 0..3 = N,E,S,W; strains 0..4 =
+ * C,D,H,S,NT. A deal is 4 hands N,E,S,W (the 32-byte input record of dd_stream,
+ * gpu/stream_main.cu:4-8). A result is 20 bytes, tricks[strain][declarer] (the payload of
+ * the 28-byte output record, gpu/stream_main.cu:298-302); E/W declarers get 13 - NS tricks
+ * also for endings with fewer than 13 cards (src/dd.h:922,937). 255 = not solved (stopped
+ * by the time limit).
+ *
+ * Every call returns DDG_OK (0) or a negative DDG_E* code; ddg_last_error() then gives a
+ * one-line message (thread-local). The reference has no error returns: its preconditions
+ * (disjoint hands of equal size 1..13, strain 0..4, TT_LOG2 >= 9) are checked here.
+ *
+ * Threading: a ddg_solver is used by one host thread at a time. Solvers on different
+ * devices are independent.
+ */
+#ifndef DDG_H
+#define DDG_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DDG_OK 0
+#define DDG_E_ARG -1     /* invalid argument or deal */
+#define DDG_E_CUDA -2    /* CUDA error (message names it) */
+#define DDG_E_MEMORY -3  /* the TT / state pool does not fit on the device */
+#define DDG_E_STATE -4   /* call out of order (e.g. stream not open) */
+#define DDG_E_TIMEOUT -5 /* a bounded device wait gave up */
+
+typedef struct ddg_solver ddg_solver;
+
+/* Solver configuration. Zero fields take the defaults. Mirrors the reference's knobs:
+ * TT_LOG2 (gpu/gpu_main.cu:192), THREADS (:202), PER_LEAD (gpu/stream_main.cu:167),
+ * TIME_LIMIT (gpu/gpu_main.cu:247). */
+typedef struct ddg_config {
+  int tt_log2;          /* TT buckets per lane = 2^tt_log2, 9..20; default 10 (320 KB per lane) */
+  int lanes;            /* solver lanes (GPU threads, one search each); default: fill the GPU */
+  int block;            /* threads per block, multiple of 32; default 128 */
+  int jobs_per_deal;    /* 5 = one job per strain, the 4 leads share a TT; 20 = one per lead */
+  int device;           /* CUDA device ordinal */
+  int schedule;         /* stage schedule of the warp loop: 0 = default */
+  double time_limit_s;  /* stop after this many seconds (unfinished results = 255); 0 = none */
+  double mem_fraction;  /* largest share of free device memory the pool may take; default 0.85 */
+} ddg_config;
+
+/* Counters of one solve call (device-side counters, summed over lanes). */
+typedef struct ddg_stats {
+  uint64_t nodes;          /* search nodes (dd_enter calls in the reference) */
+  uint64_t tt_probes;      /* TT probes */
+  uint64_t tt_hits;        /* probes that decided the node */
+  uint64_t tt_stores;      /* TT stores that reached the bucket */
+  uint64_t tt_bytes;       /* TT bytes read + written (tag lines, entries) */
+  uint64_t enter_exit[7];  /* ENTER outcomes: trivial, last trick, TT hit, quick tricks,
+                              later tricks, 2nd-hand quick tricks, expanded */
+  uint64_t stage_iters[6]; /* warp iterations per stage (TAKE, ROOT, ENTER, NEXT, RET, -) */
+  uint64_t stage_lanes[6]; /* lanes that ran the stage, summed over those iterations */
+  int64_t jobs_done;       /* finished jobs */
+  double kernel_ms;        /* device time of the solve kernel (CUDA events) */
+  int lanes;               /* lanes launched */
+  int grid, block;         /* launch shape */
+} ddg_stats;
+
+const char* ddg_version(void);
+const char* ddg_last_error(void);
+
+/* Default configuration (fills `cfg`). */
+void ddg_config_default(ddg_config* cfg);
+
+/* Creates a solver on cfg->device: allocates the per-lane TTs and search stacks once
+ * (lanes * (320 << tt_log2 + 2.6 KB) bytes) and clears the TT tags. */
+int ddg_solver_create(const ddg_config* cfg, ddg_solver** out);
+void ddg_solver_destroy(ddg_solver* s);
+/* Lanes actually allocated, and the bytes of device memory the pool holds. */
+int ddg_solver_lanes(const ddg_solver* s);
+int64_t ddg_solver_bytes(const ddg_solver* s);
+
+/* Solves n deals (hands: n*4 uint64, host memory) for all 5 strains and 4 declarers;
+ * out20: n*20 bytes, host memory. Replaces the reference's batch of dd_solve_strain calls
+ * (src/dd.h:926, cpu/cpu_main.cpp:53-68, gpu/gpu_main.cu:44-48). */
+int ddg_solve_batch(ddg_solver* s, const uint64_t* hands, int64_t n, uint8_t* out20, ddg_stats* st);
+
+/* As ddg_solve_batch, each declarer's NS tricks found by stepping from a seed
+ * (ns_seed20: n*20, NS tricks per [strain][declarer]); a right seed costs two searches.
+ * Replaces dd_solve_strain_guess (src/dd.h:915) / dd_ns_tricks_from (src/dd.h:898). */
+int ddg_solve_batch_seeded(ddg_solver* s, const uint64_t* hands, int64_t n, const int8_t* ns_seed20,
+                           uint8_t* out20, ddg_stats* st);
+
+/* Device-memory form: d_hands (n*4), d_seed20 (n*20 or NULL = binary search), d_out20
+ * (n*20), d_job_nodes (n*jobs_per_deal search nodes per job, or NULL) are device
+ * pointers; the solve is enqueued on `stream` (a cudaStream_t, NULL = legacy default)
+ * and this call waits for it. */
+int ddg_solve_device(ddg_solver* s, const uint64_t* d_hands, int64_t n, const int8_t* d_seed20,
+                     uint8_t* d_out20, uint64_t* d_job_nodes, void* stream, ddg_stats* st);
+
+/* One strain of one deal, declarers N,E,S,W (tricks as ints): the reference's
+ * dd_solve_strain (src/dd.h:926) and dd_solve_strain_guess (src/dd.h:915; ns4 = NS seeds,
+ * NULL = binary search). For many deals use ddg_solve_batch. */
+int ddg_solve_strain(ddg_solver* s, const uint64_t* hands4, int strain, const int* ns4, int* out4);
+
+/* Checks a deal (4 disjoint hands of equal size 1..13); DDG_OK or DDG_E_ARG. */
+int ddg_check_deal(const uint64_t* hands4);
+
+/* Seeded deal generator used by the command lines and the benchmarks: splitmix64 and a
+ * Fisher-Yates shuffle of the 52 cards; deal i uses its own stream, so any range can be
+ * made alone. Cards 0..4k-1 of the shuffle go round-robin to N,E,S,W (as the reference's
+ * random_deals, gpu/gpu_main.cu:154-163). hands: n*4. */
+void ddg_make_deals(uint64_t seed, int64_t first, int64_t n, int k, uint64_t* hands);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DDG_H */

@@ -27,6 +27,8 @@ struct HostEnv {
   TTBucket* tt;
   u32 mask;
   u64 start_nodes;
+  LaneStats st;
+  LaneStats& stats() { return st; }
 
   bool take(Lane& L) {
     long long job = (*next)++;
@@ -39,7 +41,7 @@ struct HostEnv {
     L.decl = jpd == 5 ? 0 : sub % 4;
     L.last_decl = jpd == 5 ? 3 : L.decl;
     L.mode = mode;
-    start_nodes = L.st.nodes;
+    start_nodes = st.nodes;
     return true;
   }
   int seed(const Lane& L) { return mode == MODE_STEP ? seeds[L.deal * 20 + L.strain * 4 + L.decl] : 7; }
@@ -47,7 +49,7 @@ struct HostEnv {
     out20[L.deal * 20 + L.strain * 4 + L.decl] = (L.decl & 1) == 0 ? ns : 13 - ns;
   }
   void job_done(const Lane& L) {
-    if (job_nodes) job_nodes[L.job] = L.st.nodes - start_nodes;
+    if (job_nodes) job_nodes[L.job] = st.nodes - start_nodes;
   }
 };
 }  // namespace
@@ -78,11 +80,12 @@ int replay_solve(const uint64_t* hands, long long n, int tt_log2, int jpd, int m
       env->next = &next;
       env->tt = tt.data();
       env->mask = (1u << tt_log2) - 1;
+      memset(&env->st, 0, sizeof(env->st));
       Lane L;
       memset(&L, 0, sizeof(L));
       L.stage = ST_TAKE;
       while (L.stage != ST_IDLE) lane_step(L, *env);
-      lane_stats[t] = L.st;
+      lane_stats[t] = env->st;
       delete env;
     });
   for (auto& th : pool) th.join();

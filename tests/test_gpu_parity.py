@@ -1,0 +1,120 @@
+"""GPU parity: the CUDA kernel against the reference's golden tables and node counts,
+called through the C ABI (libddg.so). Bit-exact tricks; node counts equal one for one
+because the search, bounds, move order and TT decisions are the reference's."""
+import numpy as np
+import pytest
+
+from conftest import load_golden
+
+pytestmark = pytest.mark.gpu
+
+
+def device_solve(ddg, solver, hands, seeds=None):
+    import torch
+    n = hands.shape[0]
+    d_h = torch.from_numpy(hands.view(np.int64)).cuda()
+    d_o = torch.empty(n * 20, dtype=torch.uint8, device="cuda")
+    d_nodes = torch.zeros(n * solver.jobs_per_deal, dtype=torch.int64, device="cuda")
+    d_s = None
+    if seeds is not None:
+        d_s = torch.from_numpy(np.ascontiguousarray(seeds, dtype=np.int8).reshape(-1)).cuda()
+    st = solver.solve_device(d_h.data_ptr(), n, d_o.data_ptr(), d_s.data_ptr() if d_s is not None else 0,
+                             d_nodes.data_ptr())
+    return d_o.cpu().numpy().reshape(n, 5, 4), d_nodes.cpu().numpy().view(np.uint64), st
+
+
+@pytest.mark.parametrize("name", [f"k{k}_120.npz" for k in range(1, 10)] + ["k6_4096.npz"])
+def test_endings_jpd5(ddg, gpu_solver, name):
+    g = load_golden(name)
+    t, nodes, st = device_solve(ddg, gpu_solver, g["hands"])
+    assert (t == g["tricks"]).all()
+    assert (nodes == g["nodes_jpd5"]).all()
+    assert st["nodes"] == int(g["nodes_jpd5"].sum())
+    assert st["jobs_done"] == g["hands"].shape[0] * 5
+
+
+@pytest.fixture(scope="module")
+def solver20(ddg):
+    s = ddg.Solver(tt_log2=10, jobs_per_deal=20, lanes=16384)
+    yield s
+    s.close()
+
+
+@pytest.mark.parametrize("name", ["k3_120.npz", "k6_4096.npz", "k9_120.npz"])
+def test_endings_jpd20(ddg, solver20, name):
+    g = load_golden(name)
+    t, nodes, st = device_solve(ddg, solver20, g["hands"])
+    assert (t == g["tricks"]).all()
+    assert (nodes == g["nodes_jpd20"]).all()
+
+
+def test_full_deals(ddg, gpu_solver):
+    g = load_golden("k13_24.npz")
+    t, nodes, st = device_solve(ddg, gpu_solver, g["hands"])
+    assert (t == g["tricks"]).all()
+    assert (nodes == g["nodes_jpd5"]).all()
+
+
+@pytest.mark.parametrize("tt", [9, 12])
+def test_tt_sizes(ddg, tt):
+    g = load_golden(f"k7_200_tt{tt}.npz")
+    s = ddg.Solver(tt_log2=tt, lanes=4096)
+    try:
+        t, nodes, _ = device_solve(ddg, s, g["hands"])
+    finally:
+        s.close()
+    assert (t == g["tricks"]).all() and (nodes == g["nodes_jpd5"]).all()
+
+
+def test_seeded_stepping(ddg, gpu_solver):
+    g = load_golden("k8_200_seeded.npz")
+    t, nodes, _ = device_solve(ddg, gpu_solver, g["hands"], g["seeds"])
+    assert (t == g["tricks"]).all() and (nodes == g["nodes_jpd5"]).all()
+
+
+def test_host_api_and_repeat_calls(ddg, gpu_solver):
+    """Host-buffer call, called twice: same tables (TT generations carry over calls)."""
+    g = load_golden("k7_120.npz")
+    a = gpu_solver.solve(g["hands"])
+    b = gpu_solver.solve(g["hands"])
+    assert (a == g["tricks"]).all() and (b == g["tricks"]).all()
+    assert gpu_solver.last_stats["nodes"] == int(g["nodes_jpd5"].sum())
+
+
+def test_generation_wrap(ddg):
+    """More than 63 jobs per lane: the TT generation wraps and the tags are cleared."""
+    g = load_golden("k5_120.npz")
+    s = ddg.Solver(tt_log2=9, lanes=64, block=64)
+    try:
+        for _ in range(3):
+            t, nodes, _ = device_solve(ddg, s, g["hands"])
+            assert (t == g["tricks"]).all() and (nodes == g["nodes_jpd5"]).all()
+    finally:
+        s.close()
+
+
+def test_solve_strain_matches_batch(ddg, gpu_solver):
+    g = load_golden("k6_120.npz")
+    for i in range(4):
+        for strain in range(5):
+            out4 = gpu_solver.solve_strain(g["hands"][i], strain)
+            assert out4 == [int(x) for x in g["tricks"][i, strain]]
+
+
+def test_empty_batch_and_bad_input(ddg, gpu_solver):
+    out = gpu_solver.solve(np.zeros((0, 4), np.uint64))
+    assert out.shape == (0, 5, 4)
+    bad = load_golden("k4_120.npz")["hands"][:3].copy()
+    bad[1, 0] = bad[1, 1]
+    with pytest.raises(ddg.DDGError):
+        gpu_solver.solve(bad)
+    with pytest.raises(ddg.DDGError):
+        gpu_solver.solve_strain(load_golden("k4_120.npz")["hands"][0], 5)
+
+
+def test_ragged_batch_sizes(ddg, gpu_solver):
+    """Batches that are not multiples of a block or warp, down to one deal."""
+    g = load_golden("k8_120.npz")
+    for n in (1, 31, 33, 97):
+        t = gpu_solver.solve(g["hands"][:n])
+        assert (t == g["tricks"][:n]).all()
