@@ -27,7 +27,8 @@ class DDGError(RuntimeError):
 class _Config(ctypes.Structure):
     _fields_ = [("tt_log2", ctypes.c_int), ("lanes", ctypes.c_int), ("block", ctypes.c_int),
                 ("jobs_per_deal", ctypes.c_int), ("device", ctypes.c_int), ("schedule", ctypes.c_int),
-                ("time_limit_s", ctypes.c_double), ("mem_fraction", ctypes.c_double)]
+                ("min_blocks", ctypes.c_int), ("time_limit_s", ctypes.c_double),
+                ("mem_fraction", ctypes.c_double)]
 
 
 class _Stats(ctypes.Structure):
@@ -69,6 +70,9 @@ def load_library():
     lib.ddg_solver_lanes.argtypes = [P]
     lib.ddg_solver_bytes.argtypes = [P]
     lib.ddg_solver_bytes.restype = ctypes.c_int64
+    lib.ddg_solver_nodes.argtypes = [P]
+    lib.ddg_solver_nodes.restype = ctypes.c_uint64
+    lib.ddg_solver_set_job_times.argtypes = [P, P]
     lib.ddg_solve_batch.argtypes = [P, P, ctypes.c_int64, P, ctypes.POINTER(_Stats)]
     lib.ddg_solve_batch_seeded.argtypes = [P, P, ctypes.c_int64, P, P, ctypes.POINTER(_Stats)]
     lib.ddg_solve_device.argtypes = [P, P, ctypes.c_int64, P, P, P, P, ctypes.POINTER(_Stats)]
@@ -102,12 +106,13 @@ class Solver:
     """A solver pool on one GPU (ddg_solver_create): per-lane TTs and stacks in HBM."""
 
     def __init__(self, tt_log2=10, lanes=0, block=128, jobs_per_deal=5, device=0, schedule=0,
-                 time_limit_s=0.0, mem_fraction=0.85):
+                 time_limit_s=0.0, mem_fraction=0.85, min_blocks=0):
         lib = load_library()
         cfg = _Config()
         lib.ddg_config_default(ctypes.byref(cfg))
         cfg.tt_log2, cfg.lanes, cfg.block = tt_log2, lanes, block
         cfg.jobs_per_deal, cfg.device, cfg.schedule = jobs_per_deal, device, schedule
+        cfg.min_blocks = min_blocks
         cfg.time_limit_s, cfg.mem_fraction = time_limit_s, mem_fraction
         self._lib = lib
         self._h = P()
@@ -158,6 +163,10 @@ class Solver:
                                           P(d_job_nodes or None), P(stream or None), ctypes.byref(st)))
         self.last_stats = st.as_dict()
         return self.last_stats
+
+    def set_job_times(self, d_job_end_ns):
+        """Device buffer (integer address, n*jobs_per_deal uint64) for job completion times."""
+        _check(self._lib.ddg_solver_set_job_times(self._h, P(d_job_end_ns or None)))
 
     def solve_strain(self, hands4, strain, ns4=None):
         """One strain of one deal, declarers N,E,S,W (the reference's dd_solve_strain)."""

@@ -35,9 +35,12 @@ int fail(int code, const char* fmt, ...) {
 
 }  // namespace
 
+struct KVariant;
+
 struct ddg_solver {
   ddg_config cfg;
   int device = 0, lanes = 0, block = 128, sms = 0;
+  const KVariant* variant = nullptr;
   TTBucket* tt = nullptr;
   Frame* stacks = nullptr;
   u32* lane_gen = nullptr;
@@ -51,6 +54,9 @@ struct ddg_solver {
   uint8_t* d_out = nullptr;
   int8_t* d_seeds = nullptr;
   int64_t cap = 0;
+  uint64_t total_nodes = 0;  // search nodes over all calls
+  uint64_t* d_job_end_ns = nullptr;  // caller's buffer for job completion times, or null
+  uint64_t start_ns = 0;             // device global timer at the last solve's launch
 };
 
 extern "C" {
@@ -85,15 +91,32 @@ int ddg_check_deal(const uint64_t* h) {
   return DDG_OK;
 }
 
-static int occupancy_blocks(int block) {
+// Compiled launch shapes: threads per block and the resident blocks per SM the register
+// allocator is held to (1 = no limit beyond the block size).
+typedef void (*BatchFn)(BatchArgs);
+struct KVariant {
+  int block, minb;
+  BatchFn fn;
+  size_t smem;  // dynamic shared memory per block
+};
+#define DDG_VARIANT(B, M) {B, M, batch_kernel<B, M>, sizeof(BlockShared<B>)}
+static const KVariant kVariants[] = {
+    DDG_VARIANT(64, 1),  DDG_VARIANT(128, 1), DDG_VARIANT(128, 4), DDG_VARIANT(128, 6), DDG_VARIANT(128, 8),
+    DDG_VARIANT(256, 1), DDG_VARIANT(256, 2), DDG_VARIANT(256, 3), DDG_VARIANT(256, 4),
+};
+#undef DDG_VARIANT
+
+static const KVariant* find_variant(int block, int minb) {
+  if (minb <= 0) minb = 1;
+  for (const KVariant& v : kVariants)
+    if (v.block == block && v.minb == minb) return &v;
+  return nullptr;
+}
+
+static int occupancy_blocks(const KVariant* v) {
   int nb = 0;
-  cudaError_t e = cudaSuccess;
-  switch (block) {
-    case 64: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, batch_kernel<64>, 64, 0); break;
-    case 128: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, batch_kernel<128>, 128, 0); break;
-    case 256: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, batch_kernel<256>, 256, 0); break;
-    default: return 0;
-  }
+  cudaError_t e = cudaFuncSetAttribute((const void*)v->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)v->smem);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, v->fn, v->block, v->smem);
   return e == cudaSuccess ? nb : 0;
 }
 
@@ -127,8 +150,10 @@ int ddg_solver_create(const ddg_config* cfg_in, ddg_solver** out) {
   }
   if (cfg.tt_log2 < TT_MIN_LOG2 || cfg.tt_log2 > 20)
     return fail(DDG_E_ARG, "tt_log2 %d is not in 9..20", cfg.tt_log2);
-  if (cfg.block != 64 && cfg.block != 128 && cfg.block != 256)
-    return fail(DDG_E_ARG, "block %d is not 64, 128 or 256", cfg.block);
+  const KVariant* variant = find_variant(cfg.block, cfg.min_blocks);
+  if (!variant)
+    return fail(DDG_E_ARG, "no kernel for block %d / min_blocks %d (64/1, 128/1,4,6,8, 256/1..4)", cfg.block,
+                cfg.min_blocks);
   if (cfg.jobs_per_deal != 5 && cfg.jobs_per_deal != 20)
     return fail(DDG_E_ARG, "jobs_per_deal %d is not 5 or 20", cfg.jobs_per_deal);
   if (cfg.lanes < 0) return fail(DDG_E_ARG, "lanes %d < 0", cfg.lanes);
@@ -140,6 +165,7 @@ int ddg_solver_create(const ddg_config* cfg_in, ddg_solver** out) {
   s->cfg = cfg;
   s->device = cfg.device;
   s->block = cfg.block;
+  s->variant = variant;
   cudaDeviceProp prop;
   cudaError_t e = cudaGetDeviceProperties(&prop, cfg.device);
   if (e != cudaSuccess) {
@@ -150,7 +176,7 @@ int ddg_solver_create(const ddg_config* cfg_in, ddg_solver** out) {
   const size_t per_lane = ((size_t)sizeof(TTBucket) << cfg.tt_log2) + sizeof(Frame) * STACK_DEPTH + 4;
   long long lanes = cfg.lanes;
   if (lanes == 0) {
-    int nb = occupancy_blocks(cfg.block);
+    int nb = occupancy_blocks(variant);
     if (nb <= 0) nb = 1;
     lanes = (long long)s->sms * nb * cfg.block;
   }
@@ -200,6 +226,13 @@ int ddg_solver_create(const ddg_config* cfg_in, ddg_solver** out) {
 }
 
 int ddg_solver_lanes(const ddg_solver* s) { return s ? s->lanes : 0; }
+
+int ddg_solver_set_job_times(ddg_solver* s, uint64_t* d_job_end_ns) {
+  if (!s) return fail(DDG_E_ARG, "null solver");
+  s->d_job_end_ns = d_job_end_ns;
+  return DDG_OK;
+}
+uint64_t ddg_solver_nodes(const ddg_solver* s) { return s ? s->total_nodes : 0; }
 int64_t ddg_solver_bytes(const ddg_solver* s) { return s ? (int64_t)s->bytes : 0; }
 
 static int launch_batch(ddg_solver* s, const BatchArgs& a, long long n_jobs, cudaStream_t stream,
@@ -208,12 +241,10 @@ static int launch_batch(ddg_solver* s, const BatchArgs& a, long long n_jobs, cud
   int grid = (int)((want + s->block - 1) / s->block);
   if (grid < 1) grid = 1;
   *grid_out = grid;
-  switch (s->block) {
-    case 64: batch_kernel<64><<<grid, 64, 0, stream>>>(a); break;
-    case 128: batch_kernel<128><<<grid, 128, 0, stream>>>(a); break;
-    default: batch_kernel<256><<<grid, 256, 0, stream>>>(a); break;
-  }
-  CUDA_TRY(cudaGetLastError());
+  BatchArgs args = a;
+  void* params[] = {&args};
+  CUDA_TRY(cudaLaunchKernel((const void*)s->variant->fn, dim3(grid), dim3(s->block), params, s->variant->smem,
+                            stream));
   return DDG_OK;
 }
 
@@ -246,6 +277,8 @@ int ddg_solve_device(ddg_solver* s, const uint64_t* d_hands, int64_t n, const in
   a.tt_log2 = s->cfg.tt_log2;
   a.schedule = s->cfg.schedule;
   a.stop = s->d_stop;
+  a.job_end_ns = s->d_job_end_ns;
+  if (s->d_job_end_ns) CUDA_TRY(cudaMemsetAsync(s->d_job_end_ns, 0, (size_t)n_jobs * 8, stream));
   CUDA_TRY(cudaEventRecord(s->ev0, stream));
   int grid = 0;
   int rc = launch_batch(s, a, n_jobs, stream, &grid);
@@ -264,9 +297,10 @@ int ddg_solve_device(ddg_solver* s, const uint64_t* d_hands, int64_t n, const in
   }
   CUDA_TRY(cudaEventSynchronize(s->ev1));
   CUDA_TRY(cudaGetLastError());
+  unsigned long long c[CNT_WORDS];
+  CUDA_TRY(cudaMemcpy(c, s->counters, sizeof(c), cudaMemcpyDeviceToHost));
+  s->total_nodes += c[CNT_NODES];
   if (st) {
-    unsigned long long c[CNT_WORDS];
-    CUDA_TRY(cudaMemcpy(c, s->counters, sizeof(c), cudaMemcpyDeviceToHost));
     st->nodes = c[CNT_NODES];
     st->tt_probes = c[CNT_PROBES];
     st->tt_hits = c[CNT_HITS];

@@ -12,8 +12,12 @@
 
 #if defined(__CUDACC__)
 #define DDG_HD __host__ __device__ __forceinline__
+// Heavy routines stay out of line on the GPU: one copy each keeps the kernel's code small
+// enough for the instruction caches, which lanes in different stages otherwise thrash.
+#define DDG_CALL __host__ __device__ __noinline__
 #else
 #define DDG_HD static inline
+#define DDG_CALL static
 #endif
 
 namespace ddg {
@@ -66,6 +70,11 @@ DDG_HD int partner_of(int h) { return (h + 2) & 3; }
 DDG_HD int rho_of(int h) { return (h + 3) & 3; }
 DDG_HD bool ns_side(int h) { return (h & 1) == 0; }
 DDG_HD int strain_trump(int strain) { return strain == 4 ? -1 : 3 - strain; }
+
+// The four hands, passed by value to out-of-line routines (eight registers).
+struct Hands {
+  u64 h[4];
+};
 
 // hands[i] for a run-time seat i, written as selects so the four hands stay in registers.
 DDG_HD u64 hand_at(const u64* h, int i) {

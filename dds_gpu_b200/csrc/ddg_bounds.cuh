@@ -29,7 +29,9 @@ DDG_HD int thrc(const Top& t, int s) { return ubyte(t.thr_c, s); }
 
 // src/dd_bounds.h:18-32: lengths from `lens`, top three cards of each suit (missing card:
 // holder -1, card 0).
-DDG_HD void top_init(Top& t, const u64* h, u64 lens) {
+DDG_CALL Top make_top(Hands hs, u64 lens) {
+  const u64* h = hs.h;
+  Top t;
   t.lens = lens;
   t.win_h = t.sec_h = t.thr_h = 0;
   t.win_c = t.sec_c = t.thr_c = 0;
@@ -37,22 +39,32 @@ DDG_HD void top_init(Top& t, const u64* h, u64 lens) {
 #pragma unroll
   for (int s = 0; s < 4; s++) {
     u64 a = all & suit_cards(s);
-    u32 hs[3], cs[3];
+    u32 who[3], crd[3];
 #pragma unroll
     for (int k = 0; k < 3; k++) {
       int c = a ? top_bit(a) : 0;
-      hs[k] = a ? (u32)holder_of(h, c) : 0xFFu;
-      cs[k] = (u32)c;
+      who[k] = a ? (u32)holder_of(h, c) : 0xFFu;
+      crd[k] = (u32)c;
       a &= ~card_bit(c);
     }
-    t.win_h |= hs[0] << (8 * s);
-    t.sec_h |= hs[1] << (8 * s);
-    t.thr_h |= hs[2] << (8 * s);
-    t.win_c |= cs[0] << (8 * s);
-    t.sec_c |= cs[1] << (8 * s);
-    t.thr_c |= cs[2] << (8 * s);
+    t.win_h |= who[0] << (8 * s);
+    t.sec_h |= who[1] << (8 * s);
+    t.thr_h |= who[2] << (8 * s);
+    t.win_c |= crd[0] << (8 * s);
+    t.sec_c |= crd[1] << (8 * s);
+    t.thr_c |= crd[2] << (8 * s);
   }
+  return t;
 }
+
+struct QtOut {  // QuickTricks: count, whether it decided the node, the cards that did
+  int q, decided;
+  u64 wr;
+};
+struct BoundOut {  // a bound's answer and the cards that decided it
+  int v;
+  u64 wr;
+};
 
 // Suit order of QuickTricks: trumps first, then the side suits in order.
 DDG_HD int qt_next_suit(int suit, int trump) {
@@ -293,7 +305,7 @@ DDG_HD int qt_blocked_sum(const Top& t, int hand, int trump, int suit, QtSuit c,
 // DDS QuickTricks for the side on lead (src/dd_bounds.h:245-438). `cutoff` = tricks the
 // leading side needs; `decided` = true when the answer is known: a count > 0 means the
 // leading side makes it, 0 that it fails (the opponents need `cutoff_other`).
-DDG_HD int quick_tricks(const u64* hands, const Top& t, int trump, int hand, int cutoff,
+DDG_HD int quick_tricks_impl(const u64* hands, const Top& t, int trump, int hand, int cutoff,
                         int cutoff_other, u64& wr, bool& decided) {
   const int P = partner_of(hand), L = lho_of(hand), R = rho_of(hand);
   int comm_card = 0, comm_suit = -1, qtricks = 0;
@@ -439,7 +451,7 @@ DDG_HD int quick_tricks(const u64* hands, const Top& t, int trump, int hand, int
 // DDS QuickTricksSecondHand (src/dd_bounds.h:442-479): can the side of `hand` (second to
 // play) win this trick and, in NT, enough more? `t` is the trick-start table (the led card
 // given back to the leader); `cutoff` counts this trick.
-DDG_HD bool quick_tricks_2nd(const u64* hands, const Top& t, int trump, int hand, int lead,
+DDG_HD bool quick_tricks_2nd_impl(const u64* hands, const Top& t, int trump, int hand, int lead,
                              int cutoff, u64& wr) {
   int ls = card_suit(lead), P = partner_of(hand), L = lho_of(hand);
   u64 S = suit_cards(ls);
@@ -500,7 +512,7 @@ DDG_HD bool others_hold(const Top& t, int wh, int s) {
 
 // DDS LaterTricksMIN (src/dd_bounds.h:482-531), NS on lead: false = NS cannot reach
 // `target` (wr = the cards that decided it).
-DDG_HD bool later_min(const Top& t, int trump, int hand, int ns_won, int left, int target,
+DDG_HD bool later_min_impl(const Top& t, int trump, int hand, int ns_won, int left, int target,
                       u64& wr) {
   int dq = left - 1;
   if (trump < 0 || winh(t, trump) < 0) {
@@ -560,7 +572,7 @@ DDG_HD bool later_min(const Top& t, int trump, int hand, int ns_won, int left, i
 }
 
 // DDS LaterTricksMAX (src/dd_bounds.h:534-584), EW on lead: true = NS reach `target`.
-DDG_HD bool later_max(const Top& t, int trump, int hand, int ns_won, int left, int target,
+DDG_HD bool later_max_impl(const Top& t, int trump, int hand, int ns_won, int left, int target,
                       u64& wr) {
   int dq = left - 1;
   if (trump < 0 || winh(t, trump) < 0) {
@@ -618,6 +630,31 @@ DDG_HD bool later_max(const Top& t, int trump, int hand, int ns_won, int left, i
     }
   }
   return false;
+}
+
+// Out-of-line entry points (arguments and results in registers).
+DDG_CALL QtOut quick_tricks(Hands hs, Top t, int trump, int hand, int cutoff, int cutoff_other) {
+  QtOut o;
+  bool d = false;
+  o.wr = 0;
+  o.q = quick_tricks_impl(hs.h, t, trump, hand, cutoff, cutoff_other, o.wr, d);
+  o.decided = d;
+  return o;
+}
+DDG_CALL BoundOut quick_tricks_2nd(Hands hs, Top t, int trump, int hand, int lead, int cutoff) {
+  BoundOut o;
+  o.wr = 0;
+  o.v = quick_tricks_2nd_impl(hs.h, t, trump, hand, lead, cutoff, o.wr);
+  return o;
+}
+// LaterTricks for the side on lead: v = 1 when the bound decides the node (NS fail when
+// NS lead, NS make it when EW lead).
+DDG_CALL BoundOut later_tricks(Top t, int trump, int leader, int ns_won, int left, int target) {
+  BoundOut o;
+  o.wr = 0;
+  o.v = ns_side(leader) ? !later_min_impl(t, trump, leader, ns_won, left, target, o.wr)
+                        : later_max_impl(t, trump, leader, ns_won, left, target, o.wr);
+  return o;
 }
 
 }  // namespace ddg

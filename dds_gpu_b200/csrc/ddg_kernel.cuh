@@ -44,12 +44,27 @@ struct BatchArgs {
   int tt_log2;
   int schedule;
   volatile int* stop;    // host-set stop flag (mapped memory), or null
+  u64* job_end_ns;       // n * jpd completion times (device global timer, ns), or null
 };
+
+__device__ __forceinline__ u64 global_ns() {
+  u64 t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
 struct LaneCounters {
   LaneStats s;
   u64 start_nodes;
-  u64 jobs_done;
+  u32 jobs_done;
+};
+
+// Dynamic shared memory of a block: lane states, counters, per-warp stage tallies.
+template <int BLOCK>
+struct BlockShared {
+  Lane lane[BLOCK];
+  LaneCounters cnt[BLOCK];
+  unsigned long long stage[BLOCK / 32][12];
 };
 
 struct DevEnv {
@@ -93,6 +108,7 @@ struct DevEnv {
   }
   __device__ __forceinline__ void job_done(const Lane& L) {
     if (a->job_nodes) a->job_nodes[L.job] = c->s.nodes - c->start_nodes;
+    if (a->job_end_ns) a->job_end_ns[L.job] = global_ns();
     c->jobs_done++;
   }
 };
@@ -106,15 +122,20 @@ __device__ __forceinline__ int pick_stage(unsigned present) {
   return ST_ENTER;
 }
 
-template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK) batch_kernel(BatchArgs a) {
-  __shared__ LaneCounters s_lane[BLOCK];
-  __shared__ unsigned long long s_stage[BLOCK / 32][12];
+// BLOCK threads per block; MINB resident blocks per SM asked of the register allocator.
+// The lane's whole search state (position, top frame, search control) is in shared
+// memory, so registers hold only the temporaries of the stage being run.
+template <int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(BatchArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  BlockShared<BLOCK>& sh = *reinterpret_cast<BlockShared<BLOCK>*>(smem_raw);
+  Lane* s_state = sh.lane;
+  LaneCounters* s_lane = sh.cnt;
+  auto& s_stage = sh.stage;
   const int tid = threadIdx.x, wid = tid >> 5, ln = tid & 31;
   const long long lane = (long long)blockIdx.x * BLOCK + tid;
   {
-    u64* z = reinterpret_cast<u64*>(&s_lane[tid]);
-    for (int k = 0; k < (int)(sizeof(LaneCounters) / 8); k++) z[k] = 0;
+    memset(&s_lane[tid], 0, sizeof(LaneCounters));
     if (ln < 12) s_stage[wid][ln] = 0;
   }
   DevEnv env;
@@ -125,7 +146,7 @@ __global__ void __launch_bounds__(BLOCK) batch_kernel(BatchArgs a) {
   env.c = &s_lane[tid];
   __syncwarp();
 
-  Lane L;
+  Lane& L = s_state[tid];
   L.stage = ST_TAKE;
   L.sp = 0;
   L.gen = a.lane_gen[lane];
@@ -164,7 +185,7 @@ __global__ void __launch_bounds__(BLOCK) batch_kernel(BatchArgs a) {
         case CNT_PROBES: sum += c.s.tt.probes; break;
         case CNT_HITS: sum += c.s.tt.hits; break;
         case CNT_STORES: sum += c.s.tt.stores; break;
-        case CNT_TT_BYTES: sum += c.s.tt.rd_bytes + c.s.tt.wr_bytes; break;
+        case CNT_TT_BYTES: sum += c.s.tt.bytes; break;
         case CNT_JOBS_DONE: sum += c.jobs_done; break;
         default:
           if (tid >= CNT_EXIT && tid < CNT_EXIT + 7) sum += c.s.enter_exit[tid - CNT_EXIT];

@@ -22,8 +22,8 @@ DDG_HD bool alike(u64 own, u64 all, int a, int b) {
 
 // Lead weight for `card` of hand `lead` (DDS weight_alloc_trump0 / weight_alloc_nt0).
 // `tt` = the card, or one alike, is the TT's best move.
-DDG_HD int lead_weight(const u64* hands, const Top& t, int trump, int left, int lead, int card,
-                       bool tt) {
+DDG_CALL int lead_weight(Hands hs, Top t, int trump, int left, int lead, int card, bool tt) {
+  const u64* hands = hs.h;
   const int s = card_suit(card), P = partner_of(lead), L = lho_of(lead), R = rho_of(lead);
   const u64 S = suit_cards(s), all = all_cards(hands);
   const u64 hP = hand_at(hands, P), hL = hand_at(hands, L), hR = hand_at(hands, R);
@@ -129,7 +129,8 @@ struct Follow {
   int high1, move1, high2, move2;  // winner (index, card) after two and after three cards
 };
 
-DDG_HD void follow_init(Follow& f, const u64* hands, int trump, int leader, u32 trick, int n) {
+DDG_HD Follow follow_init(const u64* hands, int trump, int leader, u32 trick, int n) {
+  Follow f;
   u64 th[4] = {hands[0], hands[1], hands[2], hands[3]};
   for (int i = 0; i < n; i++) toggle_card(th, (leader + i) & 3, trick_card(trick, i));
   f.lead = leader;
@@ -159,11 +160,13 @@ DDG_HD void follow_init(Follow& f, const u64* hands, int trump, int leader, u32 
   f.move1 = m1;
   f.high2 = w2;
   f.move2 = w2 == 2 ? c2 : m1;
+  return f;
 }
 
 // DDS weights for the 2nd, 3rd and 4th hand (weight_alloc_*1/2/3, without the
 // rank_forces_ace / get_top_number bonuses); n = cards played to the trick so far.
-DDG_HD int follow_weight(const Follow& f, const u64* hands, int trump, int n, int seat, int card) {
+DDG_CALL int follow_weight(Follow f, Hands hs, int trump, int n, int seat, int card) {
+  const u64* hands = hs.h;
   const int lead = f.lead, ls = f.ls, lead0 = f.lead0;
   const u64 LS = suit_cards(ls);
   const int s = card_suit(card), rank = rank2(card);

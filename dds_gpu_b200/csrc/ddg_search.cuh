@@ -85,11 +85,11 @@ DDG_HD void frame_store(Frame* p, const Frame& f) {
 #endif
 }
 
-// Search counters of one lane.
+// Search counters of one lane (per launch).
 struct LaneStats {
   u64 nodes;
   TTStats tt;
-  u64 enter_exit[7];  // trivial, last trick, TT hit, quick tricks, later tricks, QT 2nd hand, expanded
+  u32 enter_exit[7];  // trivial, last trick, TT hit, quick tricks, later tricks, QT 2nd hand, expanded
 };
 
 DDG_HD int trick_at(const Pos& p, int i) { return trick_card(p.trick, i); }
@@ -104,7 +104,9 @@ DDG_HD int winning_index(const Pos& p, int n) {
 
 // Candidate cards for `seat`, one per run of alike cards, best first (ties: higher card
 // index first). Writes them with their count into the frame.
-DDG_HD int gen_moves(const Pos& p, int seat, int hint, const Top& top, Frame& f) {
+DDG_CALL int gen_moves(const Pos& p, int seat, int hint, Top top, Frame& f) {
+  Hands hs;
+  for (int i = 0; i < 4; i++) hs.h[i] = p.h[i];
   const u64 own = hand_at(p.h, seat);
   u64 legal = own;
   u64 all = all_cards(p.h);
@@ -113,8 +115,8 @@ DDG_HD int gen_moves(const Pos& p, int seat, int hint, const Top& top, Frame& f)
     if (follow) legal = follow;
     for (int i = 0; i < p.nplayed; i++) all |= card_bit(trick_at(p, i));
   }
-  Follow fo;
-  if (p.nplayed) follow_init(fo, p.h, p.trump, p.leader, p.trick, p.nplayed);
+  Follow fo = {};
+  if (p.nplayed) fo = follow_init(p.h, p.trump, p.leader, p.trick, p.nplayed);
   u64 rest = legal & run_tops(own, all);
   int n = 0;
   int score[13];
@@ -123,8 +125,8 @@ DDG_HD int gen_moves(const Pos& p, int seat, int hint, const Top& top, Frame& f)
     int card = top_bit(rest);
     rest ^= card_bit(card);
     bool hinted = hint >= 0 && alike(own, all, hint, card);
-    int sc = p.nplayed == 0 ? lead_weight(p.h, top, p.trump, p.left, seat, card, hinted)
-                            : (hinted ? 1000 : follow_weight(fo, p.h, p.trump, p.nplayed, seat, card));
+    int sc = p.nplayed == 0 ? lead_weight(hs, top, p.trump, p.left, seat, card, hinted)
+                            : (hinted ? 1000 : follow_weight(fo, hs, p.trump, p.nplayed, seat, card));
     int i = n++;
     while (i > 0 && score[i - 1] < sc) {
       score[i] = score[i - 1];
@@ -146,11 +148,13 @@ DDG_HD int gen_moves(const Pos& p, int seat, int hint, const Top& top, Frame& f)
 
 // Enters the node at the current position (src/dd.h:626-737). Returns 0/1 when decided at
 // once (`rel` set), else -1 with `f` holding the ordered candidates.
-DDG_HD int enter(Pos& p, int target, Frame& f, u64& rel, TTBucket* tt, u32 mask, u32 gen,
-                 LaneStats& st) {
+DDG_CALL int enter(Pos& p, int target, Frame& f, u64& rel, TTBucket* tt, u32 mask, u32 gen,
+                   LaneStats& st) {
   st.nodes++;
   int need = 0, hint = -1, ub = 0;
-  Top top;
+  Top top = {};
+  Hands hs;
+  for (int i = 0; i < 4; i++) hs.h[i] = p.h[i];
   if (p.nplayed == 0) {
     rel = 0;
     if (p.ns_won >= target) {
@@ -173,49 +177,45 @@ DDG_HD int enter(Pos& p, int target, Frame& f, u64& rel, TTBucket* tt, u32 mask,
       st.enter_exit[1]++;
       return ns_side(holder_of(p.h, hi)) ? 1 : 0;
     }
-    NodeKey key;
-    make_key(key, p.h, p.leader, p.left, gen, mask);
-    int hit = tt_probe(tt, key, need, rel, hint, st.tt);
-    if (hit >= 0) {
+    const NodeKey key = make_key(hs, p.leader, p.left, gen, mask);
+    const ProbeOut pr = tt_probe(tt, key, need, st.tt);
+    hint = pr.hint;
+    if (pr.hit >= 0) {
+      rel = pr.rel;
       st.enter_exit[2]++;
-      return hit;
+      return pr.hit;
     }
     ub = p.left;
-    top_init(top, p.h, key.lens);
+    top = make_top(hs, key.lens);
     const bool ns_lead = ns_side(p.leader);
     const int cut_ns = need, cut_ew = p.left - need + 1;
-    u64 wr = 0;
-    bool decided;
-    int q = quick_tricks(p.h, top, p.trump, p.leader, ns_lead ? cut_ns : cut_ew,
-                         ns_lead ? cut_ew : cut_ns, wr, decided);
-    if (decided) {
-      bool val = ns_lead ? q != 0 : q == 0;
-      tt_store(tt, key, gen, wr, val ? need : 0, val ? p.left : need - 1, -1, st.tt);
-      rel = wr;
+    const QtOut qo = quick_tricks(hs, top, p.trump, p.leader, ns_lead ? cut_ns : cut_ew, ns_lead ? cut_ew : cut_ns);
+    if (qo.decided) {
+      bool val = ns_lead ? qo.q != 0 : qo.q == 0;
+      tt_store(tt, key, gen, qo.wr, val ? need : 0, val ? p.left : need - 1, -1, st.tt);
+      rel = qo.wr;
       st.enter_exit[3]++;
       return val ? 1 : 0;
     }
-    wr = 0;
-    bool lt = ns_lead ? !later_min(top, p.trump, p.leader, p.ns_won, p.left, target, wr)
-                      : later_max(top, p.trump, p.leader, p.ns_won, p.left, target, wr);
-    if (lt) {
+    const BoundOut lt = later_tricks(top, p.trump, p.leader, p.ns_won, p.left, target);
+    if (lt.v) {
       bool val = !ns_lead;
-      tt_store(tt, key, gen, wr, val ? need : 0, val ? p.left : need - 1, -1, st.tt);
-      rel = wr;
+      tt_store(tt, key, gen, lt.wr, val ? need : 0, val ? p.left : need - 1, -1, st.tt);
+      rel = lt.wr;
       st.enter_exit[4]++;
       return val ? 1 : 0;
     }
   } else if (p.nplayed == 1) {
     // Second hand: the trick-start table, with the led card given back to the leader.
-    u64 th[4] = {p.h[0], p.h[1], p.h[2], p.h[3]};
-    toggle_card(th, p.leader, trick_at(p, 0));
-    top_init(top, th, length_key(th));
+    Hands th = hs;
+    toggle_card(th.h, p.leader, trick_at(p, 0));
+    top = make_top(th, length_key(th.h));
     int second = lho_of(p.leader);
     int need2 = target - p.ns_won;
     int cutoff = ns_side(second) ? need2 : p.left - need2 + 1;
-    u64 wr;
-    if (quick_tricks_2nd(p.h, top, p.trump, second, trick_at(p, 0), cutoff, wr)) {
-      rel = wr;
+    const BoundOut q2 = quick_tricks_2nd(hs, top, p.trump, second, trick_at(p, 0), cutoff);
+    if (q2.v) {
+      rel = q2.wr;
       st.enter_exit[5]++;
       return ns_side(second) ? 1 : 0;
     }
@@ -271,7 +271,7 @@ DDG_HD void unplay(Pos& p, const Frame& f, int card, u64& rel) {
 
 // All moves of `f` are done (src/dd.h:772-797): widen the relevant cards through runs of
 // the hand's own touching cards, and store trick-start results in the TT.
-DDG_HD u64 finish(const Pos& p, const Frame& f, TTBucket* tt, u32 mask, u32 gen, LaneStats& st) {
+DDG_CALL u64 finish(const Pos& p, const Frame& f, TTBucket* tt, u32 mask, u32 gen, LaneStats& st) {
   u64 acc = f.acc;
   const u64 own = hand_at(p.h, fr_seat(f));
   u64 all = all_cards(p.h);
@@ -291,8 +291,9 @@ DDG_HD u64 finish(const Pos& p, const Frame& f, TTBucket* tt, u32 mask, u32 gen,
     int lb = fr_lb(f), ub = fr_ub(f);
     if (fr_result(f)) lb = fr_need(f);
     else ub = fr_need(f) - 1;
-    NodeKey key;
-    make_key(key, p.h, p.leader, p.left, gen, mask);
+    Hands hs;
+    for (int i = 0; i < 4; i++) hs.h[i] = p.h[i];
+    const NodeKey key = make_key(hs, p.leader, p.left, gen, mask);
     tt_store(tt, key, gen, acc, lb, ub, fr_best(f), st.tt);
   }
   return acc;
@@ -307,17 +308,18 @@ enum { MODE_BISECT = 0, MODE_STEP = 1 };
 // Phases of MODE_STEP: first search at the seed, stepping up, stepping down.
 enum { PH_FIRST = 0, PH_UP = 1, PH_DOWN = 2 };
 
+// A lane's whole state between stages (144 bytes; in shared memory on the GPU).
 struct Lane {
   Pos p;
-  Frame f;        // top of the stack
-  int stage, sp;  // sp = depth of f; frames 0..sp-1 are in the lane's stack
-  int target;     // the null-window search in progress: NS >= target?
-  int lo, hi;     // MODE_BISECT: answer in [lo, hi]; MODE_STEP: lo = t, hi = phase
-  int mode, decl, last_decl, strain;
+  Frame f;  // top of the stack
+  u64 r;    // relevant cards of the node just finished
   long long job, deal;
-  int v;   // value of the node just finished
-  u64 r;   // its relevant cards
   u32 gen;
+  int8_t stage, sp;  // sp = depth of f; frames 0..sp-1 are in the lane's stack
+  int8_t target;     // the null-window search in progress: NS >= target?
+  int8_t lo, hi;     // MODE_BISECT: answer in [lo, hi]; MODE_STEP: lo = t, hi = phase
+  int8_t mode, decl, last_decl, strain;
+  int8_t v;  // value of the node just finished
 };
 
 // Sets up the search of declarer `decl`'s lead (leader = decl + 1) at `target`.

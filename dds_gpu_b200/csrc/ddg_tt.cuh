@@ -34,7 +34,9 @@ struct NodeKey {
   u32 tag;      // tag without its way
 };
 
-DDG_HD void make_key(NodeKey& k, const u64* h, int leader, int left, u32 gen, u32 mask) {
+DDG_CALL NodeKey make_key(Hands hs, int leader, int left, u32 gen, u32 mask) {
+  const u64* h = hs.h;
+  NodeKey k;
   suit_codes(h, k.code);
   k.all = all_cards(h);
   k.lens = length_key(h);
@@ -42,11 +44,19 @@ DDG_HD void make_key(NodeKey& k, const u64* h, int leader, int left, u32 gen, u3
   k.bucket = (u32)x & mask;
   k.q = (x >> 9) & ((1ull << Q_BITS) - 1);
   k.tag = ((u32)(x >> 32) & 0xFFFF0000u) | ((u32)left << 12) | (gen << 2) | (u32)leader;
+  return k;
 }
 
-// Traffic counters of the TT, in bytes (what the roofline counts as algorithmic bytes).
+struct ProbeOut {  // a probe's answer (1, 0, or -1 = unknown), best-move hint, relevant cards
+  int hit, hint;
+  u64 rel;
+};
+
+// Traffic counters of the TT (bytes = what the roofline counts as algorithmic bytes).
+// Kept per launch per lane, in shared memory on the GPU.
 struct TTStats {
-  u64 probes, hits, stores, rd_bytes, wr_bytes;
+  u64 bytes;  // tag lines and entries read + written
+  u32 probes, hits, stores;
 };
 
 DDG_HD void tags_load(const TTBucket* b, u32* t) {
@@ -107,15 +117,18 @@ DDG_HD u32 tag_matches(const u32* t, u32 tag, u64& ways) {
 
 // Looks up bounds of the NS tricks still to win. Returns 1 (NS reach `need`), 0 (they do
 // not), or -1 (unknown; `hint` = the stored best move of a matching entry, if any).
-DDG_HD int tt_probe(const TTBucket* tt, const NodeKey& k, int need, u64& rel, int& hint,
-                    TTStats& st) {
+DDG_CALL ProbeOut tt_probe(const TTBucket* tt, const NodeKey& k, int need, TTStats& st) {
+  ProbeOut o;
+  o.hit = -1;
+  o.hint = -1;
+  o.rel = 0;
   const TTBucket* b = tt + k.bucket;
   u32 t[TT_WAYS];
   tags_load(b, t);
   u64 ways;
   u32 m = tag_matches(t, k.tag, ways);
   st.probes++;
-  st.rd_bytes += 64;
+  st.bytes += 64;
   int lens_s[4];
 #pragma unroll
   for (int s = 0; s < 4; s++) lens_s[s] = code_len(k.code[s]);
@@ -124,7 +137,7 @@ DDG_HD int tt_probe(const TTBucket* tt, const NodeKey& k, int need, u64& rel, in
     m &= m - 1;
     u64 w0, w1;
     entry_load(b, (int)((ways >> (4 * pos)) & 15), w0, w1);
-    st.rd_bytes += 16;
+    st.bytes += 16;
     if ((w0 & ((1ull << Q_BITS) - 1)) != k.q) continue;
     u64 owners = (w1 >> 16) | ((w0 >> 53) << 48);
     int off = 0;
@@ -148,14 +161,15 @@ DDG_HD int tt_probe(const TTBucket* tt, const NodeKey& k, int need, u64& rel, in
       u64 r = 0;
 #pragma unroll
       for (int s = 0; s < 4; s++) r |= top_n_cards(k.all, s, cnt[s]);
-      rel = r;
+      o.rel = r;
       st.hits++;
-      return lb >= need ? 1 : 0;
+      o.hit = lb >= need ? 1 : 0;
+      return o;
     }
     int bm = (int)((w0 >> (Q_BITS + 8)) & 63);
-    if (bm != 63) hint = bm;
+    if (bm != 63) o.hint = bm;
   }
-  return -1;
+  return o;
 }
 
 // Owner patterns of the relevant cards for w1 and w0's top bits; false when more than
@@ -185,14 +199,14 @@ DDG_HD u64 pack_w0(const NodeKey& k, int lb, int ub, int best, u64 hi) {
 // share `rel`'s relevant cards with this one. An entry with the same key is narrowed in
 // place; otherwise a way is taken (empty, else other generation, else least
 // 2 * tricks left + age) and its tag put in front.
-DDG_HD void tt_store(TTBucket* tt, const NodeKey& k, u32 gen, u64 rel, int lb, int ub, int best,
-                     TTStats& st) {
+DDG_CALL void tt_store(TTBucket* tt, const NodeKey& k, u32 gen, u64 rel, int lb, int ub, int best,
+                       TTStats& st) {
   u64 w1, hi;
   if (!pack_owners(k, rel, w1, hi)) return;
   TTBucket* b = tt + k.bucket;
   u32 t[TT_WAYS];
   tags_load(b, t);
-  st.rd_bytes += 64;
+  st.bytes += 64;
   st.stores++;
   u64 ways;
   u32 m = tag_matches(t, k.tag, ways);
@@ -202,7 +216,7 @@ DDG_HD void tt_store(TTBucket* tt, const NodeKey& k, u32 gen, u64 rel, int lb, i
     int way = (int)((ways >> (4 * pos)) & 15);
     u64 e0, e1;
     entry_load(b, way, e0, e1);
-    st.rd_bytes += 16;
+    st.bytes += 16;
     if ((e0 & ((1ull << Q_BITS) - 1)) == k.q && e1 == w1 && (e0 >> 53 << 53) == hi) {
       int olb = (int)((e0 >> Q_BITS) & 15), oub = (int)((e0 >> (Q_BITS + 4)) & 15);
       int obest = (int)((e0 >> (Q_BITS + 8)) & 63);
@@ -214,7 +228,7 @@ DDG_HD void tt_store(TTBucket* tt, const NodeKey& k, u32 gen, u64 rel, int lb, i
 #else
       b->e[way][0] = pack_w0(k, lb, ub, best, hi);
 #endif
-      st.wr_bytes += 8;
+      st.bytes += 8;
       return;
     }
   }
@@ -243,11 +257,11 @@ DDG_HD void tt_store(TTBucket* tt, const NodeKey& k, u32 gen, u64 rel, int lb, i
   t[0] = k.tag | ((u32)way << 8);
   tags_store(b, t);
   entry_store(b, way, pack_w0(k, lb, ub, best, hi), w1);
-  st.wr_bytes += 64 + 16;
+  st.bytes += 64 + 16;
 }
 
 // Next generation of a lane's TT; at the wrap all tags are cleared.
-DDG_HD u32 tt_next_gen(TTBucket* tt, u32 mask, u32 gen) {
+DDG_CALL u32 tt_next_gen(TTBucket* tt, u32 mask, u32 gen) {
   gen++;
   if (gen >= (1u << GEN_BITS)) {
     u32 zero[TT_WAYS];

@@ -42,7 +42,9 @@ typedef struct ddg_config {
   int block;            /* threads per block, multiple of 32; default 128 */
   int jobs_per_deal;    /* 5 = one job per strain, the 4 leads share a TT; 20 = one per lead */
   int device;           /* CUDA device ordinal */
-  int schedule;         /* stage schedule of the warp loop: 0 = default */
+  int schedule;         /* stage order of the warp loop: 0 = RET, NEXT, ROOT, TAKE, then ENTER */
+  int min_blocks;       /* resident blocks per SM the kernel is compiled for (register cap):
+                           block 128: 1, 4, 6, 8; block 256: 1..4; 0 = 1 */
   double time_limit_s;  /* stop after this many seconds (unfinished results = 255); 0 = none */
   double mem_fraction;  /* largest share of free device memory the pool may take; default 0.85 */
 } ddg_config;
@@ -77,6 +79,13 @@ void ddg_solver_destroy(ddg_solver* s);
 /* Lanes actually allocated, and the bytes of device memory the pool holds. */
 int ddg_solver_lanes(const ddg_solver* s);
 int64_t ddg_solver_bytes(const ddg_solver* s);
+/* Search nodes over all calls of this solver (the reference's DDCtx::nodes, src/dd.h:119). */
+uint64_t ddg_solver_nodes(const ddg_solver* s);
+/* Later solves write each job's completion time (device global timer, ns; 0 = not
+ * finished) into d_job_end_ns[job] (device memory, n * jobs_per_deal words, job =
+ * deal * jobs_per_deal + strain (jpd 5) or + strain * 4 + declarer (jpd 20)); NULL stops
+ * it. No counterpart in the reference, which reports no latency (per-job tails, p99). */
+int ddg_solver_set_job_times(ddg_solver* s, uint64_t* d_job_end_ns);
 
 /* Solves n deals (hands: n*4 uint64, host memory) for all 5 strains and 4 declarers;
  * out20: n*20 bytes, host memory. Replaces the reference's batch of dd_solve_strain calls

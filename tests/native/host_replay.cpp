@@ -96,7 +96,7 @@ int replay_solve(const uint64_t* hands, long long n, int tt_log2, int jpd, int m
       stats[1] += s.tt.probes;
       stats[2] += s.tt.hits;
       stats[3] += s.tt.stores;
-      stats[4] += s.tt.rd_bytes + s.tt.wr_bytes;
+      stats[4] += s.tt.bytes;
       for (int k = 0; k < 7; k++) stats[5 + k] += s.enter_exit[k];
     }
   }
