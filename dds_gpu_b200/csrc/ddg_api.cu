@@ -307,10 +307,11 @@ int ddg_solve_device(ddg_solver* s, const uint64_t* d_hands, int64_t n, const in
     st->tt_stores = c[CNT_STORES];
     st->tt_bytes = c[CNT_TT_BYTES];
     for (int k = 0; k < 7; k++) st->enter_exit[k] = c[CNT_EXIT + k];
-    for (int k = 0; k < 6; k++) {
-      st->stage_iters[k] = c[CNT_STAGE_ITERS + k];
-      st->stage_lanes[k] = c[CNT_STAGE_LANES + k];
+    for (int k = 0; k < PH_COUNT; k++) {
+      st->phase_warps[k] = c[CNT_PHASE_WARPS + k];
+      st->phase_items[k] = c[CNT_PHASE_ITEMS + k];
     }
+    st->iterations = c[CNT_ITERS];
     st->jobs_done = (int64_t)c[CNT_JOBS_DONE];
     float ms = 0;
     CUDA_TRY(cudaEventElapsedTime(&ms, s->ev0, s->ev1));

@@ -1,12 +1,17 @@
-// The batch kernel: a persistent, warp-synchronous stage machine over an atomic job queue.
+// The batch kernel: a persistent block-phase machine over an atomic job queue.
 //
-// Each thread is a solver lane with its own TT slice and frame stack in HBM; jobs
-// (one (deal, strain), or one (deal, strain, declarer)) are taken from a global counter as
-// lanes free up, so lanes that drew easy jobs keep working. In every warp iteration the
-// warp picks one stage present among its lanes (a single __reduce_or_sync of the lanes'
-// stage bits) and only the lanes in that stage run it: the cheap stages (RET, NEXT,
-// ROOT, TAKE) go first, so lanes gather at ENTER, the expensive and most divergent stage,
-// and run it together. Per-lane counters live in shared memory, not registers.
+// Each thread owns a solver lane (its own TT slice and frame stack in HBM); jobs (one
+// (deal, strain), or one (deal, strain, declarer)) come from a global counter as lanes
+// free up, so lanes that drew easy jobs keep working. The lanes' search state lives in
+// shared memory, so any thread of the block can advance any lane. Each iteration of the
+// block runs five phases in turn; a phase gathers the lanes that need it (one ballot per
+// warp, then a block-wide select) and hands them to the first threads of the block:
+//   CHEAP   returns, next moves, job starts (short, run back to back per lane)
+//   LEAD    ENTER at a trick start: TT probe, QuickTricks, LaterTricks
+//   FOLLOW  ENTER inside a trick: second-hand QuickTricks
+//   MOVES   lead / follow move generation with the DDS weights, then the first move
+// so warps run full and the whole block runs one code region at a time, instead of each
+// warp's 32 lanes scattering over the stages and branches of the search.
 #pragma once
 #include "ddg_search.cuh"
 
@@ -22,10 +27,11 @@ enum {
   CNT_HITS = 3,
   CNT_STORES = 4,
   CNT_TT_BYTES = 5,
-  CNT_EXIT = 6,          // 7 words
-  CNT_STAGE_ITERS = 13,  // 6 words
-  CNT_STAGE_LANES = 19,  // 6 words
-  CNT_JOBS_DONE = 25,
+  CNT_EXIT = 6,           // 7 words
+  CNT_PHASE_WARPS = 13,   // 8 words: warp passes per phase
+  CNT_PHASE_ITEMS = 21,   // 8 words: lanes served per phase
+  CNT_JOBS_DONE = 29,
+  CNT_ITERS = 30,         // block iterations
   CNT_WORDS = 32
 };
 
@@ -57,14 +63,6 @@ struct LaneCounters {
   LaneStats s;
   u64 start_nodes;
   u32 jobs_done;
-};
-
-// Dynamic shared memory of a block: lane states, counters, per-warp stage tallies.
-template <int BLOCK>
-struct BlockShared {
-  Lane lane[BLOCK];
-  LaneCounters cnt[BLOCK];
-  unsigned long long stage[BLOCK / 32][12];
 };
 
 struct DevEnv {
@@ -113,73 +111,133 @@ struct DevEnv {
   }
 };
 
-// Stage picked for the warp from the stages present: RET > NEXT > ROOT > TAKE > ENTER.
-__device__ __forceinline__ int pick_stage(unsigned present) {
-  if (present & (1u << ST_RET)) return ST_RET;
-  if (present & (1u << ST_NEXT)) return ST_NEXT;
-  if (present & (1u << ST_ROOT)) return ST_ROOT;
-  if (present & (1u << ST_TAKE)) return ST_TAKE;
-  return ST_ENTER;
+enum { PH_CHEAP = 0, PH_LEAD = 1, PH_FOLLOW = 2, PH_MOVES_LEAD = 3, PH_MOVES_FOLLOW = 4, PH_COUNT = 5 };
+
+template <int BLOCK>
+struct BlockShared {
+  Lane lane[BLOCK];
+  LaneCounters cnt[BLOCK];
+  BatchArgs args;
+  unsigned mask[BLOCK / 32];
+  unsigned long long ph_warps[PH_COUNT], ph_items[PH_COUNT], iters;
+  int stop;
+};
+
+// Position of the r-th (0-based) set bit of m (r < popc(m)).
+__device__ __forceinline__ int select_bit(unsigned m, int r) {
+  int pos = 0, c;
+  c = __popc(m & 0xFFFFu);
+  if (r >= c) { r -= c; m >>= 16; pos += 16; }
+  c = __popc(m & 0xFFu);
+  if (r >= c) { r -= c; m >>= 8; pos += 8; }
+  c = __popc(m & 0xFu);
+  if (r >= c) { r -= c; m >>= 4; pos += 4; }
+  c = __popc(m & 0x3u);
+  if (r >= c) { r -= c; m >>= 2; pos += 2; }
+  return pos + (r >= (int)(m & 1u) ? 1 : 0);
 }
 
-// BLOCK threads per block; MINB resident blocks per SM asked of the register allocator.
-// The lane's whole search state (position, top frame, search control) is in shared
-// memory, so registers hold only the temporaries of the stage being run.
+template <int BLOCK>
+__device__ __forceinline__ DevEnv lane_env(BlockShared<BLOCK>& sh, long long lane, int slot) {
+  DevEnv env;
+  env.a = &sh.args;
+  env.tt = sh.args.tt + (lane << sh.args.tt_log2);
+  env.mask = (1u << sh.args.tt_log2) - 1;
+  env.stack = sh.args.stacks + lane * STACK_DEPTH;
+  env.c = &sh.cnt[slot];
+  return env;
+}
+
+// One phase: the lanes that need it go, in block order, to threads 0, 1, 2, ...
+template <int BLOCK, int PH>
+__device__ __forceinline__ void run_phase(BlockShared<BLOCK>& sh, long long base, int tid) {
+  const int wid = tid >> 5, ln = tid & 31;
+  const Lane& me = sh.lane[tid];
+  bool want;
+  if (PH == PH_CHEAP) want = cheap_stage(me.stage);
+  else if (PH == PH_LEAD) want = me.stage == ST_ENTER && me.p.nplayed == 0;
+  else if (PH == PH_FOLLOW) want = me.stage == ST_ENTER && me.p.nplayed != 0;
+  else if (PH == PH_MOVES_LEAD) want = me.stage == ST_MOVES_LEAD;
+  else want = me.stage == ST_MOVES_FOLLOW;
+  const unsigned m = __ballot_sync(0xFFFFFFFFu, want);
+  if (ln == 0) sh.mask[wid] = m;
+  __syncthreads();
+  int total = 0, item = -1;
+#pragma unroll
+  for (int w = 0; w < BLOCK / 32; w++) {
+    const unsigned mw = sh.mask[w];
+    const int c = __popc(mw);
+    if (item < 0 && tid < total + c) item = w * 32 + select_bit(mw, tid - total);
+    total += c;
+  }
+  if (tid == 0 && total) {
+    sh.ph_items[PH] += total;
+    sh.ph_warps[PH] += (total + 31) >> 5;
+  }
+  if (item >= 0) {
+    DevEnv env = lane_env(sh, base + item, item);
+    Lane& L = sh.lane[item];
+    if (PH == PH_CHEAP) {
+      advance_cheap(L, env);
+    } else if (PH == PH_LEAD || PH == PH_FOLLOW) {
+      step_enter(L, env);
+    } else {
+      step_moves(L, env);
+      step_next(L, env);  // a fresh node plays its first candidate (never a skipped one)
+    }
+  }
+  __syncthreads();
+}
+
+// BLOCK threads (= lanes) per block; MINB resident blocks per SM asked of the register
+// allocator.
 template <int BLOCK, int MINB>
 __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(BatchArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   BlockShared<BLOCK>& sh = *reinterpret_cast<BlockShared<BLOCK>*>(smem_raw);
-  Lane* s_state = sh.lane;
-  LaneCounters* s_lane = sh.cnt;
-  auto& s_stage = sh.stage;
-  const int tid = threadIdx.x, wid = tid >> 5, ln = tid & 31;
-  const long long lane = (long long)blockIdx.x * BLOCK + tid;
+  const int tid = threadIdx.x;
+  const long long base = (long long)blockIdx.x * BLOCK;
+  memset(&sh.cnt[tid], 0, sizeof(LaneCounters));
   {
-    memset(&s_lane[tid], 0, sizeof(LaneCounters));
-    if (ln < 12) s_stage[wid][ln] = 0;
+    Lane& L = sh.lane[tid];
+    L.stage = ST_TAKE;
+    L.sp = 0;
+    L.gen = a.lane_gen[base + tid];
+    L.v = 0;
+    L.r = 0;
+    L.p.trick = 0;
   }
-  DevEnv env;
-  env.a = &a;
-  env.tt = a.tt + (lane << a.tt_log2);
-  env.mask = (1u << a.tt_log2) - 1;
-  env.stack = a.stacks + lane * STACK_DEPTH;
-  env.c = &s_lane[tid];
-  __syncwarp();
-
-  Lane& L = s_state[tid];
-  L.stage = ST_TAKE;
-  L.sp = 0;
-  L.gen = a.lane_gen[lane];
-  L.v = 0;
-  L.r = 0;
-  L.p.trick = 0;
-  unsigned iter = 0;
-  for (;;) {
-    const unsigned present = __reduce_or_sync(0xFFFFFFFFu, 1u << L.stage);
-    if ((present & ~(1u << ST_IDLE)) == 0) break;
-    if ((++iter & 4095u) == 0 && a.stop) {
-      int stop = __shfl_sync(0xFFFFFFFFu, ln == 0 ? *a.stop : 0, 0);
-      if (stop) {
-        L.stage = ST_IDLE;  // unfinished results stay 255
-        continue;
-      }
-    }
-    const int pick = pick_stage(present);
-    const bool run = L.stage == pick;
-    const unsigned who = __ballot_sync(0xFFFFFFFFu, run);
-    if (ln == 0) {
-      s_stage[wid][pick]++;
-      s_stage[wid][6 + pick] += __popc(who);
-    }
-    if (run) lane_step(L, env);
+  if (tid < PH_COUNT) {
+    sh.ph_warps[tid] = 0;
+    sh.ph_items[tid] = 0;
   }
-  a.lane_gen[lane] = L.gen;
+  if (tid == 0) {
+    sh.args = a;
+    sh.stop = 0;
+    sh.iters = 0;
+  }
+  __syncthreads();
+  for (unsigned iter = 0;; iter++) {
+    if (tid == 0 && a.stop && (iter & 63u) == 63u && *a.stop) sh.stop = 1;
+    if (!__syncthreads_or(sh.lane[tid].stage != ST_IDLE)) break;
+    if (sh.stop) {  // host time limit: unfinished results stay 255
+      sh.lane[tid].stage = ST_IDLE;
+      continue;
+    }
+    if (tid == 0) sh.iters++;
+    run_phase<BLOCK, PH_CHEAP>(sh, base, tid);
+    run_phase<BLOCK, PH_LEAD>(sh, base, tid);
+    run_phase<BLOCK, PH_FOLLOW>(sh, base, tid);
+    run_phase<BLOCK, PH_MOVES_LEAD>(sh, base, tid);
+    run_phase<BLOCK, PH_MOVES_FOLLOW>(sh, base, tid);
+  }
+  a.lane_gen[base + tid] = sh.lane[tid].gen;
   __syncthreads();
   // Block sums of the counters, one atomic per word per block.
   if (tid < CNT_WORDS) {
     unsigned long long sum = 0;
     for (int t = 0; t < BLOCK; t++) {
-      const LaneCounters& c = s_lane[t];
+      const LaneCounters& c = sh.cnt[t];
       switch (tid) {
         case CNT_NODES: sum += c.s.nodes; break;
         case CNT_PROBES: sum += c.s.tt.probes; break;
@@ -191,10 +249,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(BatchArgs a) {
           if (tid >= CNT_EXIT && tid < CNT_EXIT + 7) sum += c.s.enter_exit[tid - CNT_EXIT];
       }
     }
-    if (tid >= CNT_STAGE_ITERS && tid < CNT_STAGE_ITERS + 6)
-      for (int w = 0; w < BLOCK / 32; w++) sum += s_stage[w][tid - CNT_STAGE_ITERS];
-    if (tid >= CNT_STAGE_LANES && tid < CNT_STAGE_LANES + 6)
-      for (int w = 0; w < BLOCK / 32; w++) sum += s_stage[w][6 + tid - CNT_STAGE_LANES];
+    if (tid >= CNT_PHASE_WARPS && tid < CNT_PHASE_WARPS + PH_COUNT) sum = sh.ph_warps[tid - CNT_PHASE_WARPS];
+    if (tid >= CNT_PHASE_ITEMS && tid < CNT_PHASE_ITEMS + PH_COUNT) sum = sh.ph_items[tid - CNT_PHASE_ITEMS];
+    if (tid == CNT_ITERS) sum = sh.iters;
     if (tid != CNT_NEXT_JOB && sum) atomicAdd(a.counters + tid, sum);
   }
 }

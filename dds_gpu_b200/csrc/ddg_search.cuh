@@ -102,40 +102,33 @@ DDG_HD int winning_index(const Pos& p, int n) {
   return w;
 }
 
-// Candidate cards for `seat`, one per run of alike cards, best first (ties: higher card
-// index first). Writes them with their count into the frame.
-DDG_CALL int gen_moves(const Pos& p, int seat, int hint, Top top, Frame& f) {
-  Hands hs;
-  for (int i = 0; i < 4; i++) hs.h[i] = p.h[i];
+// Candidates of the hand to play: legal cards, one per run of alike cards (`all` gets
+// the cards still in play, those of the current trick included).
+DDG_HD u64 candidates(const Pos& p, int seat, u64& all) {
   const u64 own = hand_at(p.h, seat);
   u64 legal = own;
-  u64 all = all_cards(p.h);
+  all = all_cards(p.h);
   if (p.nplayed) {
     u64 follow = own & suit_cards(card_suit(trick_at(p, 0)));
     if (follow) legal = follow;
     for (int i = 0; i < p.nplayed; i++) all |= card_bit(trick_at(p, i));
   }
-  Follow fo = {};
-  if (p.nplayed) fo = follow_init(p.h, p.trump, p.leader, p.trick, p.nplayed);
-  u64 rest = legal & run_tops(own, all);
-  int n = 0;
-  int score[13];
-  int card_of[13];
-  while (rest) {
-    int card = top_bit(rest);
-    rest ^= card_bit(card);
-    bool hinted = hint >= 0 && alike(own, all, hint, card);
-    int sc = p.nplayed == 0 ? lead_weight(hs, top, p.trump, p.left, seat, card, hinted)
-                            : (hinted ? 1000 : follow_weight(fo, hs, p.trump, p.nplayed, seat, card));
-    int i = n++;
-    while (i > 0 && score[i - 1] < sc) {
-      score[i] = score[i - 1];
-      card_of[i] = card_of[i - 1];
-      i--;
-    }
-    score[i] = sc;
-    card_of[i] = card;
+  return legal & run_tops(own, all);
+}
+
+// Inserts `card` behind the candidates scoring at least `sc` (ties keep the order of
+// arrival, highest card index first), then packs the list into the frame.
+DDG_HD void insert_move(int* score, int* card_of, int& n, int card, int sc) {
+  int i = n++;
+  while (i > 0 && score[i - 1] < sc) {
+    score[i] = score[i - 1];
+    card_of[i] = card_of[i - 1];
+    i--;
   }
+  score[i] = sc;
+  card_of[i] = card;
+}
+DDG_HD void pack_moves(Frame& f, const int* card_of, int n) {
   u64 lo = 0, hi = 0;
   for (int k = 0; k < n; k++) {
     if (k < 8) lo |= (u64)card_of[k] << (8 * k);
@@ -143,76 +136,133 @@ DDG_CALL int gen_moves(const Pos& p, int seat, int hint, Top top, Frame& f) {
   }
   f.mv_lo = lo;
   f.mv_hi = hi | (u64)n << 40 | (u64)0xFF << 56;  // next index 0, no cutting card yet
-  return n;
 }
 
-// Enters the node at the current position (src/dd.h:626-737). Returns 0/1 when decided at
-// once (`rel` set), else -1 with `f` holding the ordered candidates.
-DDG_CALL int enter(Pos& p, int target, Frame& f, u64& rel, TTBucket* tt, u32 mask, u32 gen,
-                   LaneStats& st) {
-  st.nodes++;
-  int need = 0, hint = -1, ub = 0;
-  Top top = {};
+// The leader's candidates at a trick start, best first by the DDS lead weights; `hint`
+// (the TT's best move, or -1) and the cards alike to it get the weights' TT bonus.
+DDG_CALL void gen_moves_lead(const Pos& p, int hint, Top top, Frame& f) {
   Hands hs;
   for (int i = 0; i < 4; i++) hs.h[i] = p.h[i];
-  if (p.nplayed == 0) {
-    rel = 0;
-    if (p.ns_won >= target) {
-      st.enter_exit[0]++;
-      return 1;
-    }
-    if (p.ns_won + p.left < target) {
-      st.enter_exit[0]++;
-      return 0;
-    }
-    need = target - p.ns_won;
-    const u64 all = all_cards(p.h);
-    if (p.left == 1) {
-      // Last trick: the highest trump, else the highest card of the suit led.
-      int s = (p.trump >= 0 && (all & suit_cards(p.trump))) ? p.trump
-                                                            : card_suit(top_bit(hand_at(p.h, p.leader)));
-      u64 in = all & suit_cards(s);
-      int hi = top_bit(in);
-      if (popc(in) >= 2) rel = card_bit(hi);
-      st.enter_exit[1]++;
-      return ns_side(holder_of(p.h, hi)) ? 1 : 0;
-    }
-    const NodeKey key = make_key(hs, p.leader, p.left, gen, mask);
-    const ProbeOut pr = tt_probe(tt, key, need, st.tt);
-    hint = pr.hint;
-    if (pr.hit >= 0) {
-      rel = pr.rel;
-      st.enter_exit[2]++;
-      return pr.hit;
-    }
-    ub = p.left;
-    top = make_top(hs, key.lens);
-    const bool ns_lead = ns_side(p.leader);
-    const int cut_ns = need, cut_ew = p.left - need + 1;
-    const QtOut qo = quick_tricks(hs, top, p.trump, p.leader, ns_lead ? cut_ns : cut_ew, ns_lead ? cut_ew : cut_ns);
-    if (qo.decided) {
-      bool val = ns_lead ? qo.q != 0 : qo.q == 0;
-      tt_store(tt, key, gen, qo.wr, val ? need : 0, val ? p.left : need - 1, -1, st.tt);
-      rel = qo.wr;
-      st.enter_exit[3]++;
-      return val ? 1 : 0;
-    }
+  const int seat = p.leader;
+  const u64 own = hand_at(p.h, seat);
+  u64 all;
+  u64 rest = candidates(p, seat, all);
+  int n = 0, score[13], card_of[13];
+  while (rest) {
+    int card = top_bit(rest);
+    rest ^= card_bit(card);
+    bool hinted = hint >= 0 && alike(own, all, hint, card);
+    insert_move(score, card_of, n, card, lead_weight(hs, top, p.trump, p.left, seat, card, hinted));
+  }
+  pack_moves(f, card_of, n);
+}
+
+// The candidates of the 2nd, 3rd or 4th hand, best first by the DDS follow weights. (The
+// reference's TT hint never reaches these: probes happen at trick starts only.)
+DDG_CALL void gen_moves_follow(const Pos& p, Frame& f) {
+  Hands hs;
+  for (int i = 0; i < 4; i++) hs.h[i] = p.h[i];
+  const int seat = (p.leader + p.nplayed) & 3;
+  u64 all;
+  u64 rest = candidates(p, seat, all);
+  const Follow fo = follow_init(p.h, p.trump, p.leader, p.trick, p.nplayed);
+  int n = 0, score[13], card_of[13];
+  while (rest) {
+    int card = top_bit(rest);
+    rest ^= card_bit(card);
+    insert_move(score, card_of, n, card, follow_weight(fo, hs, p.trump, p.nplayed, seat, card));
+  }
+  pack_moves(f, card_of, n);
+}
+
+// Frame of a node that expands: no relevant cards or tried cards yet; `result` starts as
+// the value when no child cuts (NS to play fails, EW to play holds). The TT hint waits in
+// the frame's spare word until the moves are generated.
+DDG_HD void open_frame(Frame& f, int seat, int need, int ub, int hint) {
+  f.acc = 0;
+  f.tried = 0;
+  f.undo = 0;
+  f.pad = (u64)(uint8_t)(int8_t)hint;
+  f.info = (u32)(!ns_side(seat)) | (u32)seat << 1 | (u32)need << 3 | (u32)ub << 11 | 0xFFu << 24;
+}
+DDG_HD int frame_hint(const Frame& f) { return (int)(int8_t)(uint8_t)(f.pad & 0xFF); }
+
+// ENTER at a trick start (src/dd.h:626-705): cutoffs, the last trick, the TT probe,
+// QuickTricks and LaterTricks (their results are stored). Returns 0/1 when decided (`rel`
+// set), else -1: the node expands, `top` and the frame are ready for gen_moves_lead.
+DDG_CALL int enter_lead(Pos& p, int target, Frame& f, u64& rel, Top& top, TTBucket* tt, u32 mask, u32 gen,
+                        LaneStats& st) {
+  st.nodes++;
+  rel = 0;
+  if (p.ns_won >= target) {
+    st.enter_exit[0]++;
+    return 1;
+  }
+  if (p.ns_won + p.left < target) {
+    st.enter_exit[0]++;
+    return 0;
+  }
+  const int need = target - p.ns_won;
+  const u64 all = all_cards(p.h);
+  if (p.left == 1) {
+    // Last trick: the highest trump, else the highest card of the suit led.
+    int s = (p.trump >= 0 && (all & suit_cards(p.trump))) ? p.trump : card_suit(top_bit(hand_at(p.h, p.leader)));
+    u64 in = all & suit_cards(s);
+    int hi = top_bit(in);
+    if (popc(in) >= 2) rel = card_bit(hi);
+    st.enter_exit[1]++;
+    return ns_side(holder_of(p.h, hi)) ? 1 : 0;
+  }
+  Hands hs;
+  for (int i = 0; i < 4; i++) hs.h[i] = p.h[i];
+  const NodeKey key = make_key(hs, p.leader, p.left, gen, mask);
+  const ProbeOut pr = tt_probe(tt, key, need, st.tt);
+  if (pr.hit >= 0) {
+    rel = pr.rel;
+    st.enter_exit[2]++;
+    return pr.hit;
+  }
+  top = make_top(hs, key.lens);
+  const bool ns_lead = ns_side(p.leader);
+  const int cut_ns = need, cut_ew = p.left - need + 1;
+  const QtOut qo = quick_tricks(hs, top, p.trump, p.leader, ns_lead ? cut_ns : cut_ew, ns_lead ? cut_ew : cut_ns);
+  int val = -1;
+  u64 wr = 0;
+  if (qo.decided) {
+    val = ns_lead ? qo.q != 0 : qo.q == 0;
+    wr = qo.wr;
+    st.enter_exit[3]++;
+  } else {
     const BoundOut lt = later_tricks(top, p.trump, p.leader, p.ns_won, p.left, target);
     if (lt.v) {
-      bool val = !ns_lead;
-      tt_store(tt, key, gen, lt.wr, val ? need : 0, val ? p.left : need - 1, -1, st.tt);
-      rel = lt.wr;
+      val = !ns_lead;
+      wr = lt.wr;
       st.enter_exit[4]++;
-      return val ? 1 : 0;
     }
-  } else if (p.nplayed == 1) {
-    // Second hand: the trick-start table, with the led card given back to the leader.
-    Hands th = hs;
+  }
+  if (val >= 0) {  // one store for both bounds, so lanes that decided either way store together
+    tt_store(tt, key, gen, wr, val ? need : 0, val ? p.left : need - 1, -1, st.tt);
+    rel = wr;
+    return val;
+  }
+  open_frame(f, p.leader, need, p.left, pr.hint);
+  st.enter_exit[6]++;
+  return -1;
+}
+
+// ENTER inside a trick (src/dd.h:706-736): the second hand's QuickTricks. Returns 0/1 when
+// decided (`rel` set), else -1: the frame is ready for gen_moves_follow.
+DDG_CALL int enter_follow(Pos& p, int target, Frame& f, u64& rel, LaneStats& st) {
+  st.nodes++;
+  if (p.nplayed == 1) {
+    // The trick-start table, with the led card given back to the leader.
+    Hands hs, th;
+    for (int i = 0; i < 4; i++) hs.h[i] = th.h[i] = p.h[i];
     toggle_card(th.h, p.leader, trick_at(p, 0));
-    top = make_top(th, length_key(th.h));
-    int second = lho_of(p.leader);
-    int need2 = target - p.ns_won;
-    int cutoff = ns_side(second) ? need2 : p.left - need2 + 1;
+    const Top top = make_top(th, length_key(th.h));
+    const int second = lho_of(p.leader);
+    const int need2 = target - p.ns_won;
+    const int cutoff = ns_side(second) ? need2 : p.left - need2 + 1;
     const BoundOut q2 = quick_tricks_2nd(hs, top, p.trump, second, trick_at(p, 0), cutoff);
     if (q2.v) {
       rel = q2.wr;
@@ -220,15 +270,7 @@ DDG_CALL int enter(Pos& p, int target, Frame& f, u64& rel, TTBucket* tt, u32 mas
       return ns_side(second) ? 1 : 0;
     }
   }
-  const int seat = (p.leader + p.nplayed) & 3;
-  gen_moves(p, seat, hint, top, f);
-  f.acc = 0;
-  f.tried = 0;
-  f.undo = 0;
-  f.pad = 0;
-  // result starts as the value when no child cuts: NS to play fails, EW to play holds.
-  f.info = (u32)(!ns_side(seat)) | (u32)seat << 1 | (u32)need << 3 | (u32)0 << 7 | (u32)ub << 11 |
-           0xFFu << 24;
+  open_frame(f, (p.leader + p.nplayed) & 3, 0, 0, -1);
   st.enter_exit[6]++;
   return -1;
 }
@@ -301,7 +343,17 @@ DDG_CALL u64 finish(const Pos& p, const Frame& f, TTBucket* tt, u32 mask, u32 ge
 
 // ---- the stage machine ------------------------------------------------------------------
 
-enum Stage { ST_TAKE = 0, ST_ROOT = 1, ST_ENTER = 2, ST_NEXT = 3, ST_RET = 4, ST_IDLE = 5, ST_COUNT = 6 };
+enum Stage {
+  ST_TAKE = 0,
+  ST_ROOT = 1,
+  ST_ENTER = 2,
+  ST_NEXT = 3,
+  ST_RET = 4,
+  ST_IDLE = 5,
+  ST_MOVES_LEAD = 6,    // the node expands: generate the leader's ordered moves
+  ST_MOVES_FOLLOW = 7,  // the node expands: generate a follower's ordered moves
+  ST_COUNT = 8
+};
 
 // How a lead's trick count is found.
 enum { MODE_BISECT = 0, MODE_STEP = 1 };
@@ -312,6 +364,7 @@ enum { PH_FIRST = 0, PH_UP = 1, PH_DOWN = 2 };
 struct Lane {
   Pos p;
   Frame f;  // top of the stack
+  Top top;  // trick-start table of an expanding lead node (ENTER -> MOVES_LEAD)
   u64 r;    // relevant cards of the node just finished
   long long job, deal;
   u32 gen;
@@ -438,98 +491,140 @@ DDG_HD void node_done(Lane& L, Env& env) {
   }
 }
 
+// ---- one stage of one lane -------------------------------------------------------------
+
+template <class Env>
+DDG_HD void step_take(Lane& L, Env& env) {
+  if (!env.take(L)) {
+    L.stage = ST_IDLE;
+    return;
+  }
+  L.p.trump = strain_trump(L.strain);
+  L.p.trick = 0;
+  L.gen = tt_next_gen(env.tt, env.mask, L.gen);
+  L.stage = ST_ROOT;
+}
+
+template <class Env>
+DDG_HD void step_root(Lane& L, Env& env) {
+  start_lead(L, env.seed(L));
+  if (L.target >= 0) return;
+  // Answered without a search (a seed of 0 with no tricks left).
+  L.sp = 0;
+  L.v = 1;
+  int ans = L.lo;
+  for (;;) {
+    env.answer(L, ans);
+    L.decl++;
+    if (L.decl > L.last_decl) {
+      env.job_done(L);
+      L.stage = ST_TAKE;
+      return;
+    }
+    start_lead(L, L.mode == MODE_BISECT ? ans : env.seed(L));
+    if (L.target >= 0) return;
+    ans = L.lo;
+  }
+}
+
+// ENTER: decided at once (node done), or the node expands (moves next).
+template <class Env>
+DDG_HD void step_enter(Lane& L, Env& env) {
+  const bool lead = L.p.nplayed == 0;
+  int e = lead ? enter_lead(L.p, L.target, L.f, L.r, L.top, env.tt, env.mask, L.gen, env.stats())
+               : enter_follow(L.p, L.target, L.f, L.r, env.stats());
+  if (e < 0) {
+    L.stage = lead ? ST_MOVES_LEAD : ST_MOVES_FOLLOW;
+    return;
+  }
+  L.v = e;
+  node_done(L, env);
+}
+
+template <class Env>
+DDG_HD void step_moves(Lane& L, Env& env) {
+  if (L.stage == ST_MOVES_LEAD) gen_moves_lead(L.p, frame_hint(L.f), L.top, L.f);
+  else gen_moves_follow(L.p, L.f);
+  L.stage = ST_NEXT;
+}
+
+// NEXT: play the frame's next candidate (src/dd.h:812-835), or finish the node.
+template <class Env>
+DDG_HD void step_next(Lane& L, Env& env) {
+  Frame& f = L.f;
+  int i = fr_i(f);
+  const int n = fr_n(f);
+  while (i < n) {
+    int card = fr_move(f, i);
+    int s = card_suit(card);
+    // Cards below every relevant card of their suit are alike: one of them is tried.
+    u64 rs = f.acc & suit_cards(s);
+    u64 small = rs ? (card_bit(low_bit(rs)) - 1) & suit_cards(s) : suit_cards(s);
+    if ((small & card_bit(card)) && (small & f.tried)) {
+      i++;
+      continue;
+    }
+    fr_set_i(f, i);
+    f.tried |= card_bit(card);
+    play(L.p, f, card);
+    frame_store(env.stack + L.sp, f);
+    L.sp++;
+    L.stage = ST_ENTER;
+    return;
+  }
+  fr_set_i(f, i);
+  L.v = fr_result(f);
+  L.r = finish(L.p, f, env.tt, env.mask, L.gen, env.stats());
+  node_done(L, env);
+}
+
+// RET: the child of the top frame returned (L.v, L.r) (src/dd.h:840-854).
+template <class Env>
+DDG_HD void step_ret(Lane& L, Env& env) {
+  Frame& f = L.f;
+  int card = fr_move(f, fr_i(f));
+  unplay(L.p, f, card, L.r);
+  if (L.v == (int)ns_side(fr_seat(f))) {  // the child cuts
+    fr_set_result(f, L.v);
+    f.acc = L.r;
+    fr_set_best(f, card);
+    L.r = finish(L.p, f, env.tt, env.mask, L.gen, env.stats());
+    node_done(L, env);
+    return;
+  }
+  f.acc |= L.r;
+  fr_set_i(f, fr_i(f) + 1);
+  L.stage = ST_NEXT;
+}
+
+DDG_HD bool cheap_stage(int st) { return st == ST_RET || st == ST_NEXT || st == ST_ROOT || st == ST_TAKE; }
+
+// Runs the cheap stages back to back until the lane needs ENTER (or has no job left).
+template <class Env>
+DDG_HD void advance_cheap(Lane& L, Env& env) {
+  for (;;) {
+    switch (L.stage) {
+      case ST_RET: step_ret(L, env); break;
+      case ST_NEXT: step_next(L, env); break;
+      case ST_ROOT: step_root(L, env); break;
+      case ST_TAKE: step_take(L, env); break;
+      default: return;
+    }
+  }
+}
+
+// One stage of the lane, whatever it is (the host replay steps lanes this way).
 template <class Env>
 DDG_HD void lane_step(Lane& L, Env& env) {
   switch (L.stage) {
-    case ST_TAKE: {
-      if (!env.take(L)) {
-        L.stage = ST_IDLE;
-        return;
-      }
-      L.p.trump = strain_trump(L.strain);
-      L.p.trick = 0;
-      L.gen = tt_next_gen(env.tt, env.mask, L.gen);
-      L.stage = ST_ROOT;
-      return;
-    }
-    case ST_ROOT: {
-      start_lead(L, env.seed(L));
-      if (L.target < 0) {  // answered without a search
-        L.sp = 0;
-        L.v = 1;
-        int ans = L.lo;
-        for (;;) {
-          env.answer(L, ans);
-          L.decl++;
-          if (L.decl > L.last_decl) {
-            env.job_done(L);
-            L.stage = ST_TAKE;
-            return;
-          }
-          start_lead(L, L.mode == MODE_BISECT ? ans : env.seed(L));
-          if (L.target >= 0) return;
-          ans = L.lo;
-        }
-      }
-      return;
-    }
-    case ST_ENTER: {
-      int e = enter(L.p, L.target, L.f, L.r, env.tt, env.mask, L.gen, env.stats());
-      if (e < 0) {
-        L.stage = ST_NEXT;
-        return;
-      }
-      L.v = e;
-      node_done(L, env);
-      return;
-    }
-    case ST_NEXT: {
-      Frame& f = L.f;
-      int i = fr_i(f);
-      const int n = fr_n(f);
-      while (i < n) {
-        int card = fr_move(f, i);
-        int s = card_suit(card);
-        // Cards below every relevant card of their suit are alike: one of them is tried.
-        u64 rs = f.acc & suit_cards(s);
-        u64 small = rs ? (card_bit(low_bit(rs)) - 1) & suit_cards(s) : suit_cards(s);
-        if ((small & card_bit(card)) && (small & f.tried)) {
-          i++;
-          continue;
-        }
-        fr_set_i(f, i);
-        f.tried |= card_bit(card);
-        play(L.p, f, card);
-        frame_store(env.stack + L.sp, f);
-        L.sp++;
-        L.stage = ST_ENTER;
-        return;
-      }
-      fr_set_i(f, i);
-      L.v = fr_result(f);
-      L.r = finish(L.p, f, env.tt, env.mask, L.gen, env.stats());
-      node_done(L, env);
-      return;
-    }
-    case ST_RET: {
-      Frame& f = L.f;
-      int card = fr_move(f, fr_i(f));
-      unplay(L.p, f, card, L.r);
-      if (L.v == (int)ns_side(fr_seat(f))) {  // the child cuts
-        fr_set_result(f, L.v);
-        f.acc = L.r;
-        fr_set_best(f, card);
-        L.r = finish(L.p, f, env.tt, env.mask, L.gen, env.stats());
-        node_done(L, env);
-        return;
-      }
-      f.acc |= L.r;
-      fr_set_i(f, fr_i(f) + 1);
-      L.stage = ST_NEXT;
-      return;
-    }
-    default:
-      return;
+    case ST_TAKE: step_take(L, env); return;
+    case ST_ROOT: step_root(L, env); return;
+    case ST_ENTER: step_enter(L, env); return;
+    case ST_MOVES_LEAD:
+    case ST_MOVES_FOLLOW: step_moves(L, env); return;
+    case ST_NEXT: step_next(L, env); return;
+    case ST_RET: step_ret(L, env); return;
+    default: return;
   }
 }
 

@@ -58,8 +58,11 @@ typedef struct ddg_stats {
   uint64_t tt_bytes;       /* TT bytes read + written (tag lines, entries) */
   uint64_t enter_exit[7];  /* ENTER outcomes: trivial, last trick, TT hit, quick tricks,
                               later tricks, 2nd-hand quick tricks, expanded */
-  uint64_t stage_iters[6]; /* warp iterations per stage (TAKE, ROOT, ENTER, NEXT, RET, -) */
-  uint64_t stage_lanes[6]; /* lanes that ran the stage, summed over those iterations */
+  uint64_t phase_warps[5]; /* warp passes per phase of the block loop: cheap stages, ENTER at
+                              a trick start, ENTER inside a trick, lead moves, follow moves */
+  uint64_t phase_items[5]; /* lanes served by those passes; items / (32 * warps) is the
+                              phase's warp efficiency */
+  uint64_t iterations;     /* block iterations, summed over blocks */
   int64_t jobs_done;       /* finished jobs */
   double kernel_ms;        /* device time of the solve kernel (CUDA events) */
   int lanes;               /* lanes launched */
