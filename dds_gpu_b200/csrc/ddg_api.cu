@@ -74,6 +74,7 @@ void ddg_config_default(ddg_config* c) {
   c->schedule = 0;
   c->time_limit_s = 0;
   c->mem_fraction = 0.85;
+  c->help = 0;
 }
 
 int ddg_check_deal(const uint64_t* h) {
@@ -278,6 +279,7 @@ int ddg_solve_device(ddg_solver* s, const uint64_t* d_hands, int64_t n, const in
   a.schedule = s->cfg.schedule;
   a.stop = s->d_stop;
   a.job_end_ns = s->d_job_end_ns;
+  a.help = s->cfg.help;
   if (s->d_job_end_ns) CUDA_TRY(cudaMemsetAsync(s->d_job_end_ns, 0, (size_t)n_jobs * 8, stream));
   CUDA_TRY(cudaEventRecord(s->ev0, stream));
   int grid = 0;
@@ -312,6 +314,7 @@ int ddg_solve_device(ddg_solver* s, const uint64_t* d_hands, int64_t n, const in
       st->phase_items[k] = c[CNT_PHASE_ITEMS + k];
     }
     st->iterations = c[CNT_ITERS];
+    st->tasks = c[CNT_TASKS];
     st->jobs_done = (int64_t)c[CNT_JOBS_DONE];
     float ms = 0;
     CUDA_TRY(cudaEventElapsedTime(&ms, s->ev0, s->ev1));

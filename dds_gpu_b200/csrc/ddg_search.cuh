@@ -69,7 +69,7 @@ DDG_HD void frame_load(Frame& f, const Frame* p) {
   f.mv_hi = b.y;
   f.undo = (u32)c.x;
   f.info = (u32)(c.x >> 32);
-  f.pad = 0;
+  f.pad = c.y;
 #else
   f = *p;
 #endif
@@ -79,7 +79,7 @@ DDG_HD void frame_store(Frame* p, const Frame& f) {
   ulonglong2* v = reinterpret_cast<ulonglong2*>(p);
   v[0] = make_ulonglong2(f.acc, f.tried);
   v[1] = make_ulonglong2(f.mv_lo, f.mv_hi);
-  v[2] = make_ulonglong2((u64)f.undo | ((u64)f.info << 32), 0);
+  v[2] = make_ulonglong2((u64)f.undo | ((u64)f.info << 32), f.pad);
 #else
   *p = f;
 #endif
@@ -186,6 +186,15 @@ DDG_HD void open_frame(Frame& f, int seat, int need, int ub, int hint) {
   f.info = (u32)(!ns_side(seat)) | (u32)seat << 1 | (u32)need << 3 | (u32)ub << 11 | 0xFFu << 24;
 }
 DDG_HD int frame_hint(const Frame& f) { return (int)(int8_t)(uint8_t)(f.pad & 0xFF); }
+// The spare word also records a donation: bits 32..47 = task id + 1 (0 = none), bits
+// 48..55 = the frame's candidate count before its tail was donated.
+DDG_HD int fr_task(const Frame& f) { return (int)((f.pad >> 32) & 0xFFFF) - 1; }
+DDG_HD int fr_full_n(const Frame& f) { return (int)((f.pad >> 48) & 0xFF); }
+DDG_HD void fr_set_n(Frame& f, int n) { fr_set_hi_byte(f, 13, n); }
+DDG_HD void fr_set_task(Frame& f, int task, int full_n) {
+  f.pad = (f.pad & 0xFFFFFFFFull) | ((u64)(task + 1) << 32) | ((u64)full_n << 48);
+}
+DDG_HD void fr_clear_task(Frame& f) { f.pad &= 0xFFFFFFFFull; }
 
 // ENTER at a trick start (src/dd.h:626-705): cutoffs, the last trick, the TT probe,
 // QuickTricks and LaterTricks (their results are stored). Returns 0/1 when decided (`rel`
@@ -341,6 +350,125 @@ DDG_CALL u64 finish(const Pos& p, const Frame& f, TTBucket* tt, u32 mask, u32 ge
   return acc;
 }
 
+// ---- helping: tasks of donated sibling moves ---------------------------------------------
+//
+// When the job queue is empty, lanes without work (HUNGRY) help busy lanes of their block.
+// A busy lane donates the untried candidates of its shallowest frame whose first child was
+// searched without a cutoff (a node likely to need all its children); a helper searches
+// them from that frame's position, with its own TT, and reports the value of that part:
+// a cutoff (value, the cutting child's relevant cards and card), or no cutoff (the union of
+// the children's relevant cards). The donor merges the part into the frame when its own
+// children are done, exactly as if it had searched them itself: cutoffs are exact, and a
+// card skipped as a small card is skipped on the evidence of a child whose relevant cards
+// are in the frame's set. Node counts then differ from the sequential search; tricks do not.
+// A donor never waits on a task nobody has taken (it takes the moves back), so every wait
+// is on a lane that is searching, and the block always finishes.
+enum { TASK_FREE = 0, TASK_QUEUED = 1, TASK_RUNNING = 2, TASK_DONE = 3, TASK_ABANDONED = 4, TASK_FILLING = 5 };
+enum { MAX_TASKS = 64, MAX_DONATE_DEPTH = 28 };
+
+struct Task {
+  Pos pos;          // position at the donated frame, before its next candidate
+  u64 mv_lo, mv_hi;  // the donated candidates, packed as in a frame (count in byte 13)
+  u64 acc, tried;   // the donor frame's relevant and tried cards at the donation
+  u64 r;            // result: relevant cards of the donated part
+  u32 info;         // the donor frame's info word (seat, result so far)
+  int8_t target;    // the null-window target of the donor's search
+  int8_t v;         // result: value of the donated part
+  int8_t best;      // result: the cutting card, or -1
+};
+
+struct TaskPool {
+  Task t[MAX_TASKS];
+  int state[MAX_TASKS];
+  int queued;  // tasks in TASK_QUEUED
+  int posted;  // tasks posted so far
+};
+
+DDG_HD int atom_cas(int* p, int cmp, int val) {
+#ifdef __CUDA_ARCH__
+  return atomicCAS(p, cmp, val);
+#else
+  int old = *p;
+  if (old == cmp) *p = val;
+  return old;
+#endif
+}
+DDG_HD void atom_add(int* p, int v) {
+#ifdef __CUDA_ARCH__
+  atomicAdd(p, v);
+#else
+  *p += v;
+#endif
+}
+DDG_HD int atom_load(const int* p) {
+#ifdef __CUDA_ARCH__
+  return *(const volatile int*)p;
+#else
+  return *p;
+#endif
+}
+DDG_HD void fence_block() {
+#ifdef __CUDA_ARCH__
+  __threadfence_block();
+#endif
+}
+
+// Publishes a task; its id, or -1 when the pool is full.
+DDG_HD int task_post(TaskPool& tp, const Task& t) {
+  for (int k = 0; k < MAX_TASKS; k++) {
+    if (atom_load(&tp.state[k]) != TASK_FREE || atom_cas(&tp.state[k], TASK_FREE, TASK_FILLING) != TASK_FREE)
+      continue;
+    tp.t[k] = t;
+    fence_block();
+    atom_cas(&tp.state[k], TASK_FILLING, TASK_QUEUED);
+    atom_add(&tp.queued, 1);
+    atom_add(&tp.posted, 1);
+    return k;
+  }
+  return -1;
+}
+DDG_HD int task_claim(TaskPool& tp) {
+  if (atom_load(&tp.queued) <= 0) return -1;
+  for (int k = 0; k < MAX_TASKS; k++) {
+    if (atom_load(&tp.state[k]) == TASK_QUEUED && atom_cas(&tp.state[k], TASK_QUEUED, TASK_RUNNING) == TASK_QUEUED) {
+      atom_add(&tp.queued, -1);
+      fence_block();
+      return k;
+    }
+  }
+  return -1;
+}
+// Takes an unclaimed task back; true when it was still queued.
+DDG_HD bool task_retract(TaskPool& tp, int k) {
+  if (atom_cas(&tp.state[k], TASK_QUEUED, TASK_FREE) == TASK_QUEUED) {
+    atom_add(&tp.queued, -1);
+    return true;
+  }
+  return false;
+}
+// The helper's result; a task abandoned meanwhile is simply freed.
+DDG_HD void task_finish(TaskPool& tp, int k, int v, u64 r, int best) {
+  tp.t[k].v = (int8_t)v;
+  tp.t[k].r = r;
+  tp.t[k].best = (int8_t)best;
+  fence_block();
+  if (atom_cas(&tp.state[k], TASK_RUNNING, TASK_DONE) != TASK_RUNNING) tp.state[k] = TASK_FREE;
+}
+// The donor no longer needs the task (its own part cut off).
+DDG_HD void task_abandon(TaskPool& tp, int k) {
+  for (;;) {
+    int s = atom_load(&tp.state[k]);
+    if (s == TASK_QUEUED) {
+      if (task_retract(tp, k)) return;
+    } else if (s == TASK_RUNNING) {
+      if (atom_cas(&tp.state[k], TASK_RUNNING, TASK_ABANDONED) == TASK_RUNNING) return;
+    } else {  // done: free it (abandoned or free already: nothing to do)
+      if (s == TASK_DONE) atom_cas(&tp.state[k], TASK_DONE, TASK_FREE);
+      return;
+    }
+  }
+}
+
 // ---- the stage machine ------------------------------------------------------------------
 
 enum Stage {
@@ -352,7 +480,9 @@ enum Stage {
   ST_IDLE = 5,
   ST_MOVES_LEAD = 6,    // the node expands: generate the leader's ordered moves
   ST_MOVES_FOLLOW = 7,  // the node expands: generate a follower's ordered moves
-  ST_COUNT = 8
+  ST_HUNGRY = 8,        // no job left: waits for a task of its block to help with
+  ST_WAIT = 9,          // a frame's own children are done; its donated part is still running
+  ST_COUNT = 10
 };
 
 // How a lead's trick count is found.
@@ -360,7 +490,7 @@ enum { MODE_BISECT = 0, MODE_STEP = 1 };
 // Phases of MODE_STEP: first search at the seed, stepping up, stepping down.
 enum { PH_FIRST = 0, PH_UP = 1, PH_DOWN = 2 };
 
-// A lane's whole state between stages (144 bytes; in shared memory on the GPU).
+// A lane's whole state between stages (192 bytes; in shared memory on the GPU).
 struct Lane {
   Pos p;
   Frame f;  // top of the stack
@@ -368,6 +498,7 @@ struct Lane {
   u64 r;    // relevant cards of the node just finished
   long long job, deal;
   u32 gen;
+  int16_t task;      // the task this lane helps with, or -1 (its own job)
   int8_t stage, sp;  // sp = depth of f; frames 0..sp-1 are in the lane's stack
   int8_t target;     // the null-window search in progress: NS >= target?
   int8_t lo, hi;     // MODE_BISECT: answer in [lo, hi]; MODE_STEP: lo = t, hi = phase
@@ -492,13 +623,19 @@ DDG_HD void node_done(Lane& L, Env& env) {
 }
 
 // ---- one stage of one lane -------------------------------------------------------------
+//
+// Besides the members listed above node_done, an Env offers helping:
+//   TaskPool* pool()        the block's tasks, or null when helping is off
+//   bool want_donation()    lanes of the block are hungry and no task is waiting for them
+//   bool block_done()       no job is left and no lane of the block is busy
 
 template <class Env>
 DDG_HD void step_take(Lane& L, Env& env) {
   if (!env.take(L)) {
-    L.stage = ST_IDLE;
+    L.stage = env.pool() ? ST_HUNGRY : ST_IDLE;
     return;
   }
+  L.task = -1;
   L.p.trump = strain_trump(L.strain);
   L.p.trick = 0;
   L.gen = tt_next_gen(env.tt, env.mask, L.gen);
@@ -548,34 +685,75 @@ DDG_HD void step_moves(Lane& L, Env& env) {
   L.stage = ST_NEXT;
 }
 
+// The top frame is done with value L.v: a helper's task root reports to its donor (no
+// widening, no TT store: the frame holds only part of the node's moves); any other
+// frame is finished and returns to its parent.
+template <class Env>
+DDG_HD void frame_done(Lane& L, Env& env) {
+  Frame& f = L.f;
+  if (L.sp == 0 && L.task >= 0) {
+    task_finish(*env.pool(), L.task, L.v, f.acc, fr_best(f));
+    L.task = -1;
+    L.stage = ST_HUNGRY;
+    return;
+  }
+  L.r = finish(L.p, f, env.tt, env.mask, L.gen, env.stats());
+  node_done(L, env);
+}
+
 // NEXT: play the frame's next candidate (src/dd.h:812-835), or finish the node.
 template <class Env>
 DDG_HD void step_next(Lane& L, Env& env) {
   Frame& f = L.f;
-  int i = fr_i(f);
-  const int n = fr_n(f);
-  while (i < n) {
-    int card = fr_move(f, i);
-    int s = card_suit(card);
-    // Cards below every relevant card of their suit are alike: one of them is tried.
-    u64 rs = f.acc & suit_cards(s);
-    u64 small = rs ? (card_bit(low_bit(rs)) - 1) & suit_cards(s) : suit_cards(s);
-    if ((small & card_bit(card)) && (small & f.tried)) {
-      i++;
-      continue;
+  for (;;) {
+    int i = fr_i(f);
+    const int n = fr_n(f);
+    while (i < n) {
+      int card = fr_move(f, i);
+      int s = card_suit(card);
+      // Cards below every relevant card of their suit are alike: one of them is tried.
+      u64 rs = f.acc & suit_cards(s);
+      u64 small = rs ? (card_bit(low_bit(rs)) - 1) & suit_cards(s) : suit_cards(s);
+      if ((small & card_bit(card)) && (small & f.tried)) {
+        i++;
+        continue;
+      }
+      fr_set_i(f, i);
+      f.tried |= card_bit(card);
+      play(L.p, f, card);
+      frame_store(env.stack + L.sp, f);
+      L.sp++;
+      L.stage = ST_ENTER;
+      return;
     }
     fr_set_i(f, i);
-    f.tried |= card_bit(card);
-    play(L.p, f, card);
-    frame_store(env.stack + L.sp, f);
-    L.sp++;
-    L.stage = ST_ENTER;
-    return;
+    const int t = fr_task(f);
+    if (t < 0) break;
+    // Own children done; the donated tail decides what comes next.
+    TaskPool& tp = *env.pool();
+    if (task_retract(tp, t)) {  // nobody took it: search it here after all
+      fr_set_n(f, fr_full_n(f));
+      fr_clear_task(f);
+      continue;
+    }
+    if (atom_load(&tp.state[t]) != TASK_DONE) {
+      L.stage = ST_WAIT;
+      return;
+    }
+    const Task& k = tp.t[t];
+    if (k.v == (int)ns_side(fr_seat(f))) {  // the donated part cut off
+      fr_set_result(f, k.v);
+      f.acc = k.r;
+      fr_set_best(f, k.best);
+    } else {
+      f.acc |= k.r;
+    }
+    tp.state[t] = TASK_FREE;
+    fr_clear_task(f);
+    break;
   }
-  fr_set_i(f, i);
   L.v = fr_result(f);
-  L.r = finish(L.p, f, env.tt, env.mask, L.gen, env.stats());
-  node_done(L, env);
+  frame_done(L, env);
 }
 
 // RET: the child of the top frame returned (L.v, L.r) (src/dd.h:840-854).
@@ -585,11 +763,15 @@ DDG_HD void step_ret(Lane& L, Env& env) {
   int card = fr_move(f, fr_i(f));
   unplay(L.p, f, card, L.r);
   if (L.v == (int)ns_side(fr_seat(f))) {  // the child cuts
+    const int t = fr_task(f);
+    if (t >= 0) {  // the donated tail is not needed any more
+      task_abandon(*env.pool(), t);
+      fr_clear_task(f);
+    }
     fr_set_result(f, L.v);
     f.acc = L.r;
     fr_set_best(f, card);
-    L.r = finish(L.p, f, env.tt, env.mask, L.gen, env.stats());
-    node_done(L, env);
+    frame_done(L, env);
     return;
   }
   f.acc |= L.r;
@@ -597,17 +779,133 @@ DDG_HD void step_ret(Lane& L, Env& env) {
   L.stage = ST_NEXT;
 }
 
-DDG_HD bool cheap_stage(int st) { return st == ST_RET || st == ST_NEXT || st == ST_ROOT || st == ST_TAKE; }
+// WAIT: the top frame's donated tail is running on a helper.
+template <class Env>
+DDG_HD bool step_wait(Lane& L, Env& env) {
+  if (atom_load(&env.pool()->state[fr_task(L.f)]) != TASK_DONE) return false;
+  L.stage = ST_NEXT;  // NEXT merges the result and finishes the frame
+  return true;
+}
 
-// Runs the cheap stages back to back until the lane needs ENTER (or has no job left).
+// HUNGRY: take a task of the block, or stop when nothing is left to do.
+template <class Env>
+DDG_HD bool step_hungry(Lane& L, Env& env) {
+  TaskPool& tp = *env.pool();
+  const int t = task_claim(tp);
+  if (t < 0) {
+    if (env.block_done()) L.stage = ST_IDLE;
+    return false;
+  }
+  const Task& k = tp.t[t];
+  L.p = k.pos;
+  L.f.acc = k.acc;
+  L.f.tried = k.tried;
+  L.f.mv_lo = k.mv_lo;
+  L.f.mv_hi = k.mv_hi;
+  L.f.undo = 0;
+  L.f.info = k.info;
+  L.f.pad = 0;
+  L.sp = 0;
+  L.target = k.target;
+  L.task = (int16_t)t;
+  L.gen = tt_next_gen(env.tt, env.mask, L.gen);
+  L.stage = ST_NEXT;
+  return true;
+}
+
+// A helper whose task was abandoned stops, and abandons what it had donated itself.
+template <class Env>
+DDG_HD void abort_task(Lane& L, Env& env) {
+  TaskPool& tp = *env.pool();
+  for (int k = 0; k < L.sp; k++) {
+    Frame g;
+    frame_load(g, env.stack + k);
+    if (fr_task(g) >= 0) task_abandon(tp, fr_task(g));
+  }
+  // In NEXT, RET and WAIT the top frame is the one at depth sp; in ENTER and MOVES it is
+  // the copy of frame sp-1 (done above) or a fresh frame without a task.
+  const bool top_is_own = L.stage == ST_NEXT || L.stage == ST_RET || L.stage == ST_WAIT;
+  if (top_is_own && fr_task(L.f) >= 0) task_abandon(tp, fr_task(L.f));
+  tp.state[L.task] = TASK_FREE;
+  L.task = -1;
+  L.stage = ST_HUNGRY;
+}
+DDG_HD bool task_abandoned(const Lane& L, const TaskPool* tp) {
+  return L.task >= 0 && atom_load(&tp->state[L.task]) == TASK_ABANDONED;
+}
+
+// Donates the untried tail of the shallowest frame (below the top) whose first child was
+// searched without a cutoff. The lane is in NEXT, so its position is that of the top
+// frame; the donated frame's position is found by taking back the moves above it.
+template <class Env>
+DDG_HD bool try_donate(Lane& L, Env& env) {
+  const int top = L.sp < MAX_DONATE_DEPTH ? L.sp : MAX_DONATE_DEPTH;
+  for (int d = 0; d < top; d++) {
+    Frame g;
+    frame_load(g, env.stack + d);
+    const int i = fr_i(g), n = fr_n(g);
+    if (fr_task(g) >= 0 || i < 1 || n - i < 2) continue;
+    Task t;
+    t.pos = L.p;
+    for (int j = L.sp - 1; j >= d; j--) {
+      Frame h;
+      if (j == d) h = g;
+      else frame_load(h, env.stack + j);
+      u64 dummy = 0;
+      unplay(t.pos, h, fr_move(h, fr_i(h)), dummy);
+    }
+    int cards[13], m = 0;
+    for (int k = i + 1; k < n; k++) cards[m++] = fr_move(g, k);
+    Frame tail;
+    pack_moves(tail, cards, m);
+    t.mv_lo = tail.mv_lo;
+    t.mv_hi = tail.mv_hi;
+    // The child the donor is still searching counts as not tried for the helper: its
+    // relevant cards are not in acc yet, so it cannot justify skipping a small card.
+    t.acc = g.acc;
+    t.tried = g.tried & ~card_bit(fr_move(g, i));
+    t.info = g.info;
+    t.target = L.target;
+    t.r = 0;
+    t.v = 0;
+    t.best = -1;
+    const int id = task_post(*env.pool(), t);
+    if (id < 0) return false;
+    fr_set_task(g, id, n);
+    fr_set_n(g, i + 1);
+    frame_store(env.stack + d, g);
+    return true;
+  }
+  return false;
+}
+
+DDG_HD bool cheap_stage(int st) {
+  return st == ST_RET || st == ST_NEXT || st == ST_ROOT || st == ST_TAKE || st == ST_HUNGRY || st == ST_WAIT;
+}
+
+// Runs the cheap stages back to back until the lane needs ENTER, waits, or has nothing
+// left. A lane about to play its next move first donates when its block is hungry.
 template <class Env>
 DDG_HD void advance_cheap(Lane& L, Env& env) {
+  bool offered = false;
   for (;;) {
     switch (L.stage) {
       case ST_RET: step_ret(L, env); break;
-      case ST_NEXT: step_next(L, env); break;
+      case ST_NEXT:
+        if (!offered && env.pool() && env.want_donation() && L.sp > 0) {
+          offered = true;
+          try_donate(L, env);
+        }
+        step_next(L, env);
+        break;
       case ST_ROOT: step_root(L, env); break;
       case ST_TAKE: step_take(L, env); break;
+      case ST_WAIT:
+        if (!step_wait(L, env)) return;
+        break;
+      case ST_HUNGRY:
+        if (!step_hungry(L, env)) return;
+        break;
       default: return;
     }
   }
@@ -624,6 +922,8 @@ DDG_HD void lane_step(Lane& L, Env& env) {
     case ST_MOVES_FOLLOW: step_moves(L, env); return;
     case ST_NEXT: step_next(L, env); return;
     case ST_RET: step_ret(L, env); return;
+    case ST_WAIT: step_wait(L, env); return;
+    case ST_HUNGRY: step_hungry(L, env); return;
     default: return;
   }
 }

@@ -47,6 +47,9 @@ typedef struct ddg_config {
                            block 128: 1, 4, 6, 8; block 256: 1..4; 0 = 1 */
   double time_limit_s;  /* stop after this many seconds (unfinished results = 255); 0 = none */
   double mem_fraction;  /* largest share of free device memory the pool may take; default 0.85 */
+  int help;             /* 1: once the job queue is empty, idle lanes take over untried sibling
+                           moves of busy lanes in their block (same tricks, other node counts);
+                           0: every job is searched by one lane, nodes equal the reference's */
 } ddg_config;
 
 /* Counters of one solve call (device-side counters, summed over lanes). */
@@ -63,6 +66,7 @@ typedef struct ddg_stats {
   uint64_t phase_items[5]; /* lanes served by those passes; items / (32 * warps) is the
                               phase's warp efficiency */
   uint64_t iterations;     /* block iterations, summed over blocks */
+  uint64_t tasks;          /* sibling-move tasks handed to helping lanes */
   int64_t jobs_done;       /* finished jobs */
   double kernel_ms;        /* device time of the solve kernel (CUDA events) */
   int lanes;               /* lanes launched */

@@ -29,6 +29,9 @@ struct HostEnv {
   u64 start_nodes;
   LaneStats st;
   LaneStats& stats() { return st; }
+  TaskPool* pool() { return nullptr; }
+  bool want_donation() { return false; }
+  bool block_done() { return true; }
 
   bool take(Lane& L) {
     long long job = (*next)++;
@@ -54,7 +57,116 @@ struct HostEnv {
 };
 }  // namespace
 
+// A block of lanes stepped through the GPU kernel's phases in order (one lane at a time),
+// with the block's task pool: the helping logic (donation, retraction, merging,
+// abandonment) runs exactly as on the GPU, deterministically.
+struct SimShared {
+  TaskPool pool;
+  int budget = 0;
+  bool exhausted = false;
+  int busy = 0;
+};
+struct SimEnv : HostEnv {
+  SimShared* sh;
+  TaskPool* pool() { return &sh->pool; }
+  bool want_donation() {
+    if (sh->budget <= 0) return false;
+    sh->budget--;
+    return true;
+  }
+  bool block_done() { return sh->exhausted && sh->busy == 0; }
+  bool take(Lane& L) {
+    if (!HostEnv::take(L)) {
+      sh->exhausted = true;
+      return false;
+    }
+    return true;
+  }
+};
+
+static bool busy_stage(int st) { return st != ST_HUNGRY && st != ST_IDLE; }
+
 extern "C" {
+// n deals on one simulated block of `lanes` lanes, with helping; `eager` donates whenever a
+// lane could (not only when lanes are hungry). Results and nodes as replay_solve; stats[12]
+// = tasks posted, stats[13] = block iterations.
+int replay_block(const uint64_t* hands, long long n, int tt_log2, int jpd, int lanes, int eager, int* out20,
+                 uint64_t* stats) {
+  if (tt_log2 < TT_MIN_LOG2 || tt_log2 > 16 || (jpd != 5 && jpd != 20) || lanes < 1 || lanes > 1024) return -1;
+  std::atomic<long long> next{0};
+  SimShared* sh = new SimShared();
+  memset(&sh->pool, 0, sizeof(sh->pool));
+  std::vector<SimEnv*> envs(lanes);
+  std::vector<std::vector<TTBucket>> tts(lanes);
+  std::vector<Lane> L(lanes);
+  for (int i = 0; i < lanes; i++) {
+    tts[i].assign((size_t)1 << tt_log2, TTBucket());
+    memset(tts[i].data(), 0, tts[i].size() * sizeof(TTBucket));
+    SimEnv* e = new SimEnv();
+    e->hands = hands;
+    e->n_jobs = n * jpd;
+    e->jpd = jpd;
+    e->mode = MODE_BISECT;
+    e->seeds = nullptr;
+    e->out20 = out20;
+    e->job_nodes = nullptr;
+    e->next = &next;
+    e->tt = tts[i].data();
+    e->mask = (1u << tt_log2) - 1;
+    memset(&e->st, 0, sizeof(e->st));
+    e->sh = sh;
+    envs[i] = e;
+    memset(&L[i], 0, sizeof(Lane));
+    L[i].stage = ST_TAKE;
+    L[i].task = -1;
+  }
+  uint64_t iters = 0;
+  for (;;) {
+    int hungry = 0, busy = 0, live = 0;
+    for (int i = 0; i < lanes; i++) {
+      hungry += L[i].stage == ST_HUNGRY;
+      busy += busy_stage(L[i].stage);
+      live += L[i].stage != ST_IDLE;
+    }
+    if (!live) break;
+    if (++iters > 4000000000ull) return -2;
+    sh->busy = busy;
+    sh->budget = eager ? lanes : hungry - sh->pool.queued;
+    for (int i = 0; i < lanes; i++) {  // CHEAP (with abandoned helpers)
+      if (task_abandoned(L[i], &sh->pool)) abort_task(L[i], *envs[i]);
+      if (cheap_stage(L[i].stage)) advance_cheap(L[i], *envs[i]);
+    }
+    for (int i = 0; i < lanes; i++)
+      if (L[i].stage == ST_ENTER && L[i].p.nplayed == 0) step_enter(L[i], *envs[i]);
+    for (int i = 0; i < lanes; i++)
+      if (L[i].stage == ST_ENTER && L[i].p.nplayed != 0) step_enter(L[i], *envs[i]);
+    for (int ph = ST_MOVES_LEAD; ph <= ST_MOVES_FOLLOW; ph++)
+      for (int i = 0; i < lanes; i++)
+        if (L[i].stage == ph) {
+          step_moves(L[i], *envs[i]);
+          step_next(L[i], *envs[i]);
+        }
+  }
+  for (int k = 0; k < MAX_TASKS; k++)
+    if (sh->pool.state[k] != TASK_FREE) return -3;  // every task must be back in the pool
+  if (stats) {
+    memset(stats, 0, 14 * sizeof(uint64_t));
+    for (auto* e : envs) {
+      stats[0] += e->st.nodes;
+      stats[1] += e->st.tt.probes;
+      stats[2] += e->st.tt.hits;
+      stats[3] += e->st.tt.stores;
+      stats[4] += e->st.tt.bytes;
+    }
+    stats[12] = (uint64_t)sh->pool.posted;
+    stats[13] = iters;
+  }
+  for (auto* e : envs) delete e;
+  delete sh;
+  return 0;
+}
+
+
 // n deals, jpd 5 or 20 jobs per deal, mode 0 (binary search) / 1 (stepping from seeds).
 // stats[0..4] = nodes, probes, hits, stores, TT bytes; stats[5..11] = enter exits.
 int replay_solve(const uint64_t* hands, long long n, int tt_log2, int jpd, int mode,

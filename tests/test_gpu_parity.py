@@ -123,3 +123,29 @@ def test_ragged_batch_sizes(ddg, gpu_solver):
     for n in (1, 31, 33, 97):
         t = gpu_solver.solve(g["hands"][:n])
         assert (t == g["tricks"][:n]).all()
+
+
+@pytest.fixture(scope="module")
+def helper_solver(ddg):
+    s = ddg.Solver(tt_log2=10, jobs_per_deal=20, lanes=1024, block=256, min_blocks=2, help=1, time_limit_s=120)
+    yield s
+    s.close()
+
+
+@pytest.mark.parametrize("name", ["k5_120.npz", "k7_120.npz", "k9_120.npz", "k6_4096.npz"])
+def test_helping_exact_tricks(ddg, helper_solver, name):
+    """With helping on, idle lanes take over sibling moves of busy lanes: node counts change,
+    every trick count must still equal the reference's."""
+    g = load_golden(name)
+    t, _, st = device_solve(ddg, helper_solver, g["hands"])
+    assert (t == g["tricks"]).all()
+    assert st["jobs_done"] == g["hands"].shape[0] * 20
+
+
+def test_helping_splits_hard_deals(ddg, helper_solver):
+    """Few full deals on many lanes: lanes go hungry at once and take donated moves."""
+    g = load_golden("k13_24.npz")
+    hands = np.ascontiguousarray(g["hands"][LIGHT_13])
+    t, _, st = device_solve(ddg, helper_solver, hands)
+    assert (t == g["tricks"][LIGHT_13]).all()
+    assert st["tasks"] > 0
