@@ -57,6 +57,7 @@ struct ddg_solver {
   uint64_t total_nodes = 0;  // search nodes over all calls
   uint64_t* d_job_end_ns = nullptr;  // caller's buffer for job completion times, or null
   uint64_t start_ns = 0;             // device global timer at the last solve's launch
+  TaskPool* tasks = nullptr;         // helping's task pool (cfg.help), cleared per solve
 };
 
 extern "C" {
@@ -128,6 +129,7 @@ void ddg_solver_destroy(ddg_solver* s) {
   cudaFree(s->stacks);
   cudaFree(s->lane_gen);
   cudaFree(s->counters);
+  cudaFree(s->tasks);
   cudaFree(s->d_hands);
   cudaFree(s->d_out);
   cudaFree(s->d_seeds);
@@ -176,10 +178,16 @@ int ddg_solver_create(const ddg_config* cfg_in, ddg_solver** out) {
   s->sms = prop.multiProcessorCount;
   const size_t per_lane = ((size_t)sizeof(TTBucket) << cfg.tt_log2) + sizeof(Frame) * STACK_DEPTH + 4;
   long long lanes = cfg.lanes;
-  if (lanes == 0) {
-    int nb = occupancy_blocks(variant);
-    if (nb <= 0) nb = 1;
-    lanes = (long long)s->sms * nb * cfg.block;
+  int nb = occupancy_blocks(variant);  // also sets the kernel's dynamic shared memory limit
+  if (nb <= 0) {
+    delete s;
+    return fail(DDG_E_CUDA, "kernel variant %d/%d does not fit on an SM", cfg.block, cfg.min_blocks);
+  }
+  const long long resident = (long long)s->sms * nb * cfg.block;
+  if (lanes == 0) lanes = resident;
+  if (cfg.help && lanes > resident) {
+    delete s;
+    return fail(DDG_E_ARG, "helping needs every block resident: at most %lld lanes", resident);
   }
   size_t free_b = 0, total_b = 0;
   e = cudaMemGetInfo(&free_b, &total_b);
@@ -208,6 +216,7 @@ int ddg_solver_create(const ddg_config* cfg_in, ddg_solver** out) {
   if (e == cudaSuccess) e = cudaMalloc(&s->stacks, st_bytes);
   if (e == cudaSuccess) e = cudaMalloc(&s->lane_gen, (size_t)lanes * 4);
   if (e == cudaSuccess) e = cudaMalloc(&s->counters, CNT_WORDS * 8);
+  if (e == cudaSuccess && cfg.help) e = cudaMalloc(&s->tasks, sizeof(TaskPool));
   if (e == cudaSuccess) e = cudaMemset(s->tt, 0, tt_bytes);
   if (e == cudaSuccess) e = cudaMemset(s->lane_gen, 0, (size_t)lanes * 4);
   if (e == cudaSuccess) e = cudaHostAlloc(&s->h_stop, sizeof(int), cudaHostAllocMapped);
@@ -238,7 +247,8 @@ int64_t ddg_solver_bytes(const ddg_solver* s) { return s ? (int64_t)s->bytes : 0
 
 static int launch_batch(ddg_solver* s, const BatchArgs& a, long long n_jobs, cudaStream_t stream,
                         int* grid_out) {
-  long long want = n_jobs < s->lanes ? n_jobs : s->lanes;
+  // With helping every resident lane is launched: lanes without a job help the others.
+  long long want = (a.tasks || n_jobs > s->lanes) ? s->lanes : n_jobs;
   int grid = (int)((want + s->block - 1) / s->block);
   if (grid < 1) grid = 1;
   *grid_out = grid;
@@ -279,7 +289,8 @@ int ddg_solve_device(ddg_solver* s, const uint64_t* d_hands, int64_t n, const in
   a.schedule = s->cfg.schedule;
   a.stop = s->d_stop;
   a.job_end_ns = s->d_job_end_ns;
-  a.help = s->cfg.help;
+  a.tasks = s->tasks;
+  if (s->tasks) CUDA_TRY(cudaMemsetAsync(s->tasks, 0, sizeof(TaskPool), stream));
   if (s->d_job_end_ns) CUDA_TRY(cudaMemsetAsync(s->d_job_end_ns, 0, (size_t)n_jobs * 8, stream));
   CUDA_TRY(cudaEventRecord(s->ev0, stream));
   int grid = 0;
@@ -314,7 +325,12 @@ int ddg_solve_device(ddg_solver* s, const uint64_t* d_hands, int64_t n, const in
       st->phase_items[k] = c[CNT_PHASE_ITEMS + k];
     }
     st->iterations = c[CNT_ITERS];
-    st->tasks = c[CNT_TASKS];
+    st->tasks = 0;
+    if (s->tasks) {
+      int posted = 0;
+      CUDA_TRY(cudaMemcpy(&posted, &s->tasks->posted, sizeof(int), cudaMemcpyDeviceToHost));
+      st->tasks = (uint64_t)posted;
+    }
     st->jobs_done = (int64_t)c[CNT_JOBS_DONE];
     float ms = 0;
     CUDA_TRY(cudaEventElapsedTime(&ms, s->ev0, s->ev1));

@@ -52,7 +52,7 @@ struct BatchArgs {
   int schedule;
   volatile int* stop;    // host-set stop flag (mapped memory), or null
   u64* job_end_ns;       // n * jpd completion times (device global timer, ns), or null
-  int help;              // idle lanes help busy lanes of their block (tricks exact, nodes differ)
+  TaskPool* tasks;       // helping: idle lanes take donated moves (tricks exact), or null
 };
 
 __device__ __forceinline__ u64 global_ns() {
@@ -67,34 +67,32 @@ struct LaneCounters {
   u32 jobs_done;
 };
 
-// Block-wide state of helping (shared memory).
-struct HelpState {
-  TaskPool pool;
-  int budget;     // donations still wanted this iteration
-  int busy;       // lanes with a job or a task at the start of the iteration
-  int exhausted;  // the job queue is empty
-};
-
 struct DevEnv {
   const BatchArgs* a;
   Frame* stack;
   TTBucket* tt;
   u32 mask;
   LaneCounters* c;
-  HelpState* hs;  // null when helping is off
+  TaskPool* tp;           // null when helping is off
+  const int* help_hint;   // block flag: hungry lanes outnumber queued tasks (this iteration)
+  long long lane;
 
   __device__ __forceinline__ LaneStats& stats() { return c->s; }
-  __device__ __forceinline__ TaskPool* pool() { return hs ? &hs->pool : nullptr; }
-  __device__ __forceinline__ bool want_donation() { return atomicSub(&hs->budget, 1) > 0; }
-  __device__ __forceinline__ bool block_done() {
-    return *(volatile int*)&hs->exhausted && *(volatile int*)&hs->busy == 0;
+  __device__ __forceinline__ TaskPool* pool() { return tp; }
+  __device__ __forceinline__ bool want_donation() {
+    if (!*help_hint) return false;
+    const int q = atomicAdd(&tp->queued, 1);
+    if (q < atom_load(&tp->hungry)) return true;
+    atomicAdd(&tp->queued, -1);
+    return false;
   }
+  __device__ __forceinline__ void unreserve() { atomicAdd(&tp->queued, -1); }
+  __device__ __forceinline__ int claim_start() { return (int)((lane * 61) + (global_ns() >> 12)); }
+  __device__ __forceinline__ u64 work_nodes() { return c->s.nodes - c->start_nodes; }
+  __device__ __forceinline__ void task_started() { c->start_nodes = c->s.nodes; }
   __device__ __forceinline__ bool take(Lane& L) {
     unsigned long long job = atomicAdd(a->counters + CNT_NEXT_JOB, 1ull);
-    if ((long long)job >= a->n_jobs) {
-      if (hs) hs->exhausted = 1;
-      return false;
-    }
+    if ((long long)job >= a->n_jobs) return false;
     L.job = (long long)job;
     L.deal = L.job / a->jpd;
     int sub = (int)(L.job - L.deal * a->jpd);
@@ -136,11 +134,11 @@ template <int BLOCK>
 struct BlockShared {
   Lane lane[BLOCK];
   LaneCounters cnt[BLOCK];
-  HelpState help;
   BatchArgs args;
   unsigned mask[BLOCK / 32];
   unsigned long long ph_warps[PH_COUNT], ph_items[PH_COUNT], iters;
   int stop;
+  int help_hint;  // hungry lanes outnumber queued tasks (read once per iteration)
 };
 
 // Position of the r-th (0-based) set bit of m (r < popc(m)).
@@ -165,7 +163,9 @@ __device__ __forceinline__ DevEnv lane_env(BlockShared<BLOCK>& sh, long long lan
   env.mask = (1u << sh.args.tt_log2) - 1;
   env.stack = sh.args.stacks + lane * STACK_DEPTH;
   env.c = &sh.cnt[slot];
-  env.hs = sh.args.help ? &sh.help : nullptr;
+  env.tp = sh.args.tasks;
+  env.help_hint = &sh.help_hint;
+  env.lane = lane;
   return env;
 }
 
@@ -175,7 +175,7 @@ __device__ __forceinline__ void run_phase(BlockShared<BLOCK>& sh, long long base
   const int wid = tid >> 5, ln = tid & 31;
   const Lane& me = sh.lane[tid];
   bool want;
-  if (PH == PH_CHEAP) want = cheap_stage(me.stage) || (sh.args.help && task_abandoned(me, &sh.help.pool));
+  if (PH == PH_CHEAP) want = cheap_stage(me.stage) || (sh.args.tasks && task_abandoned(me, sh.args.tasks));
   else if (PH == PH_LEAD) want = me.stage == ST_ENTER && me.p.nplayed == 0;
   else if (PH == PH_FOLLOW) want = me.stage == ST_ENTER && me.p.nplayed != 0;
   else if (PH == PH_MOVES_LEAD) want = me.stage == ST_MOVES_LEAD;
@@ -199,7 +199,7 @@ __device__ __forceinline__ void run_phase(BlockShared<BLOCK>& sh, long long base
     DevEnv env = lane_env(sh, base + item, item);
     Lane& L = sh.lane[item];
     if (PH == PH_CHEAP) {
-      if (env.hs && task_abandoned(L, &sh.help.pool)) abort_task(L, env);
+      if (env.tp && task_abandoned(L, env.tp)) abort_task(L, env);
       advance_cheap(L, env);
     } else if (PH == PH_LEAD || PH == PH_FOLLOW) {
       step_enter(L, env);
@@ -230,7 +230,6 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(BatchArgs a) {
     L.p.trick = 0;
     L.task = -1;
   }
-  for (int k = tid; k < MAX_TASKS; k += BLOCK) sh.help.pool.state[k] = TASK_FREE;
   if (tid < PH_COUNT) {
     sh.ph_warps[tid] = 0;
     sh.ph_items[tid] = 0;
@@ -239,11 +238,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(BatchArgs a) {
     sh.args = a;
     sh.stop = 0;
     sh.iters = 0;
-    sh.help.pool.queued = 0;
-    sh.help.pool.posted = 0;
-    sh.help.budget = 0;
-    sh.help.busy = 0;
-    sh.help.exhausted = 0;
+    sh.help_hint = 0;
   }
   __syncthreads();
   for (unsigned iter = 0;; iter++) {
@@ -253,16 +248,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(BatchArgs a) {
       sh.lane[tid].stage = ST_IDLE;
       continue;
     }
-    if (tid == 0) sh.iters++;
-    if (a.help) {
-      const int st = sh.lane[tid].stage;
-      const int hungry = __syncthreads_count(st == ST_HUNGRY);
-      const int busy = __syncthreads_count(st != ST_HUNGRY && st != ST_IDLE);
-      if (tid == 0) {
-        sh.help.busy = busy;
-        sh.help.budget = hungry - sh.help.pool.queued;
-      }
-      __syncthreads();
+    if (tid == 0) {
+      sh.iters++;
+      if (a.tasks) sh.help_hint = atom_load(&a.tasks->hungry) > atom_load(&a.tasks->queued);
     }
     run_phase<BLOCK, PH_CHEAP>(sh, base, tid);
     run_phase<BLOCK, PH_LEAD>(sh, base, tid);
@@ -291,7 +279,6 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(BatchArgs a) {
     if (tid >= CNT_PHASE_WARPS && tid < CNT_PHASE_WARPS + PH_COUNT) sum = sh.ph_warps[tid - CNT_PHASE_WARPS];
     if (tid >= CNT_PHASE_ITEMS && tid < CNT_PHASE_ITEMS + PH_COUNT) sum = sh.ph_items[tid - CNT_PHASE_ITEMS];
     if (tid == CNT_ITERS) sum = sh.iters;
-    if (tid == CNT_TASKS) sum = (unsigned long long)sh.help.pool.posted;
     if (tid != CNT_NEXT_JOB && sum) atomicAdd(a.counters + tid, sum);
   }
 }

@@ -352,19 +352,20 @@ DDG_CALL u64 finish(const Pos& p, const Frame& f, TTBucket* tt, u32 mask, u32 ge
 
 // ---- helping: tasks of donated sibling moves ---------------------------------------------
 //
-// When the job queue is empty, lanes without work (HUNGRY) help busy lanes of their block.
-// A busy lane donates the untried candidates of its shallowest frame whose first child was
-// searched without a cutoff (a node likely to need all its children); a helper searches
-// them from that frame's position, with its own TT, and reports the value of that part:
-// a cutoff (value, the cutting child's relevant cards and card), or no cutoff (the union of
-// the children's relevant cards). The donor merges the part into the frame when its own
-// children are done, exactly as if it had searched them itself: cutoffs are exact, and a
-// card skipped as a small card is skipped on the evidence of a child whose relevant cards
-// are in the frame's set. Node counts then differ from the sequential search; tricks do not.
-// A donor never waits on a task nobody has taken (it takes the moves back), so every wait
-// is on a lane that is searching, and the block always finishes.
+// When the job queue is empty, lanes without work (HUNGRY) help busy lanes, on any SM. A
+// lane whose job has run a while donates the untried candidates of its shallowest frame
+// whose first child was searched without a cutoff (a node likely to need all its
+// children); a helper searches them from that frame's position, with its own TT, and
+// reports the value of that part: a cutoff (value, the cutting child's relevant cards and
+// card), or no cutoff (the union of the children's relevant cards). The donor merges the
+// part into the frame when its own children are done, exactly as if it had searched them
+// itself: cutoffs are exact, and a card skipped as a small card is skipped on the evidence
+// of a child whose relevant cards are in the frame's set. Node counts then differ from the
+// sequential search; tricks do not. A donor never waits on a task nobody has taken (it
+// takes the moves back), and waits are checked once per block iteration, never spun on:
+// every wait is on a lane that is searching in a resident block, so the launch finishes.
 enum { TASK_FREE = 0, TASK_QUEUED = 1, TASK_RUNNING = 2, TASK_DONE = 3, TASK_ABANDONED = 4, TASK_FILLING = 5 };
-enum { MAX_TASKS = 64, MAX_DONATE_DEPTH = 28 };
+enum { MAX_TASKS = 1024, CLAIM_WINDOW = 64, MAX_DONATE_DEPTH = 28, DONATE_MIN_NODES = 4096 };
 
 struct Task {
   Pos pos;          // position at the donated frame, before its next candidate
@@ -377,11 +378,15 @@ struct Task {
   int8_t best;      // result: the cutting card, or -1
 };
 
+// The tasks of a launch and the counters that steer helping (HBM on the GPU).
 struct TaskPool {
   Task t[MAX_TASKS];
   int state[MAX_TASKS];
-  int queued;  // tasks in TASK_QUEUED
-  int posted;  // tasks posted so far
+  int queued;     // tasks queued, or reserved by a donor about to post one
+  int posted;     // tasks posted so far
+  int hungry;     // lanes waiting for a task
+  int busy;       // lanes holding a job or a task
+  int exhausted;  // the job queue is empty
 };
 
 DDG_HD int atom_cas(int* p, int cmp, int val) {
@@ -409,27 +414,30 @@ DDG_HD int atom_load(const int* p) {
 }
 DDG_HD void fence_block() {
 #ifdef __CUDA_ARCH__
-  __threadfence_block();
+  __threadfence();  // task records travel between SMs
 #endif
 }
 
-// Publishes a task; its id, or -1 when the pool is full.
-DDG_HD int task_post(TaskPool& tp, const Task& t) {
-  for (int k = 0; k < MAX_TASKS; k++) {
+// Publishes a task (its `queued` slot was reserved by the donor); its id, or -1 when the
+// pool is full. The search for a free slot starts at `start` to spread donors out.
+DDG_HD int task_post(TaskPool& tp, const Task& t, int start) {
+  for (int j = 0; j < MAX_TASKS; j++) {
+    const int k = (start + j) & (MAX_TASKS - 1);
     if (atom_load(&tp.state[k]) != TASK_FREE || atom_cas(&tp.state[k], TASK_FREE, TASK_FILLING) != TASK_FREE)
       continue;
     tp.t[k] = t;
     fence_block();
     atom_cas(&tp.state[k], TASK_FILLING, TASK_QUEUED);
-    atom_add(&tp.queued, 1);
     atom_add(&tp.posted, 1);
     return k;
   }
   return -1;
 }
-DDG_HD int task_claim(TaskPool& tp) {
+// Takes a queued task from a window of the pool starting at `start`; its id, or -1.
+DDG_HD int task_claim(TaskPool& tp, int start) {
   if (atom_load(&tp.queued) <= 0) return -1;
-  for (int k = 0; k < MAX_TASKS; k++) {
+  for (int j = 0; j < CLAIM_WINDOW; j++) {
+    const int k = (start + j) & (MAX_TASKS - 1);
     if (atom_load(&tp.state[k]) == TASK_QUEUED && atom_cas(&tp.state[k], TASK_QUEUED, TASK_RUNNING) == TASK_QUEUED) {
       atom_add(&tp.queued, -1);
       fence_block();
@@ -612,6 +620,7 @@ DDG_HD void node_done(Lane& L, Env& env) {
     L.decl++;
     if (L.decl > L.last_decl) {
       env.job_done(L);
+      if (env.pool()) atom_add(&env.pool()->busy, -1);
       L.stage = ST_TAKE;
       return;
     }
@@ -625,16 +634,26 @@ DDG_HD void node_done(Lane& L, Env& env) {
 // ---- one stage of one lane -------------------------------------------------------------
 //
 // Besides the members listed above node_done, an Env offers helping:
-//   TaskPool* pool()        the block's tasks, or null when helping is off
-//   bool want_donation()    lanes of the block are hungry and no task is waiting for them
-//   bool block_done()       no job is left and no lane of the block is busy
+//   TaskPool* pool()        the launch's tasks and helping counters, or null (helping off)
+//   bool want_donation()    a hungry lane has no task waiting for it: reserves one
+//   void unreserve()        gives back a reservation that was not used
+//   int claim_start()       where this lane starts looking for a task in the pool
+//   u64 work_nodes()        nodes searched since the lane's job or task began
 
 template <class Env>
 DDG_HD void step_take(Lane& L, Env& env) {
+  TaskPool* tp = env.pool();
   if (!env.take(L)) {
-    L.stage = env.pool() ? ST_HUNGRY : ST_IDLE;
+    if (tp) {
+      tp->exhausted = 1;
+      atom_add(&tp->hungry, 1);
+      L.stage = ST_HUNGRY;
+    } else {
+      L.stage = ST_IDLE;
+    }
     return;
   }
+  if (tp) atom_add(&tp->busy, 1);
   L.task = -1;
   L.p.trump = strain_trump(L.strain);
   L.p.trick = 0;
@@ -655,6 +674,7 @@ DDG_HD void step_root(Lane& L, Env& env) {
     L.decl++;
     if (L.decl > L.last_decl) {
       env.job_done(L);
+      if (env.pool()) atom_add(&env.pool()->busy, -1);
       L.stage = ST_TAKE;
       return;
     }
@@ -692,8 +712,11 @@ template <class Env>
 DDG_HD void frame_done(Lane& L, Env& env) {
   Frame& f = L.f;
   if (L.sp == 0 && L.task >= 0) {
-    task_finish(*env.pool(), L.task, L.v, f.acc, fr_best(f));
+    TaskPool& tp = *env.pool();
+    task_finish(tp, L.task, L.v, f.acc, fr_best(f));
     L.task = -1;
+    atom_add(&tp.busy, -1);
+    atom_add(&tp.hungry, 1);
     L.stage = ST_HUNGRY;
     return;
   }
@@ -791,11 +814,17 @@ DDG_HD bool step_wait(Lane& L, Env& env) {
 template <class Env>
 DDG_HD bool step_hungry(Lane& L, Env& env) {
   TaskPool& tp = *env.pool();
-  const int t = task_claim(tp);
+  const int t = task_claim(tp, env.claim_start());
   if (t < 0) {
-    if (env.block_done()) L.stage = ST_IDLE;
+    if (atom_load(&tp.exhausted) && atom_load(&tp.busy) == 0) {  // nothing left anywhere
+      atom_add(&tp.hungry, -1);
+      L.stage = ST_IDLE;
+    }
     return false;
   }
+  atom_add(&tp.hungry, -1);
+  atom_add(&tp.busy, 1);
+  env.task_started();
   const Task& k = tp.t[t];
   L.p = k.pos;
   L.f.acc = k.acc;
@@ -828,6 +857,8 @@ DDG_HD void abort_task(Lane& L, Env& env) {
   if (top_is_own && fr_task(L.f) >= 0) task_abandon(tp, fr_task(L.f));
   tp.state[L.task] = TASK_FREE;
   L.task = -1;
+  atom_add(&tp.busy, -1);
+  atom_add(&tp.hungry, 1);
   L.stage = ST_HUNGRY;
 }
 DDG_HD bool task_abandoned(const Lane& L, const TaskPool* tp) {
@@ -869,7 +900,7 @@ DDG_HD bool try_donate(Lane& L, Env& env) {
     t.r = 0;
     t.v = 0;
     t.best = -1;
-    const int id = task_post(*env.pool(), t);
+    const int id = task_post(*env.pool(), t, env.claim_start());
     if (id < 0) return false;
     fr_set_task(g, id, n);
     fr_set_n(g, i + 1);
@@ -892,9 +923,9 @@ DDG_HD void advance_cheap(Lane& L, Env& env) {
     switch (L.stage) {
       case ST_RET: step_ret(L, env); break;
       case ST_NEXT:
-        if (!offered && env.pool() && env.want_donation() && L.sp > 0) {
+        if (!offered && env.pool() && L.sp > 0 && env.work_nodes() >= DONATE_MIN_NODES && env.want_donation()) {
           offered = true;
-          try_donate(L, env);
+          if (!try_donate(L, env)) env.unreserve();
         }
         step_next(L, env);
         break;

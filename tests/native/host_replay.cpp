@@ -31,7 +31,10 @@ struct HostEnv {
   LaneStats& stats() { return st; }
   TaskPool* pool() { return nullptr; }
   bool want_donation() { return false; }
-  bool block_done() { return true; }
+  void unreserve() {}
+  int claim_start() { return 0; }
+  u64 work_nodes() { return st.nodes - start_nodes; }
+  void task_started() { start_nodes = st.nodes; }
 
   bool take(Lane& L) {
     long long job = (*next)++;
@@ -62,29 +65,24 @@ struct HostEnv {
 // abandonment) runs exactly as on the GPU, deterministically.
 struct SimShared {
   TaskPool pool;
-  int budget = 0;
-  bool exhausted = false;
-  int busy = 0;
+  int budget = 0;  // donations allowed this iteration
+  bool eager = false;
 };
 struct SimEnv : HostEnv {
   SimShared* sh;
+  int lane_id = 0, min_nodes = 0;
   TaskPool* pool() { return &sh->pool; }
   bool want_donation() {
-    if (sh->budget <= 0) return false;
+    if (sh->budget <= 0 || (!sh->eager && sh->pool.queued >= sh->pool.hungry)) return false;
     sh->budget--;
+    sh->pool.queued++;
     return true;
   }
-  bool block_done() { return sh->exhausted && sh->busy == 0; }
-  bool take(Lane& L) {
-    if (!HostEnv::take(L)) {
-      sh->exhausted = true;
-      return false;
-    }
-    return true;
-  }
+  void unreserve() { sh->pool.queued--; }
+  int claim_start() { return lane_id * 61; }
+  u64 work_nodes() { return st.nodes - start_nodes + (u64)DONATE_MIN_NODES - (u64)min_nodes; }
 };
 
-static bool busy_stage(int st) { return st != ST_HUNGRY && st != ST_IDLE; }
 
 extern "C" {
 // n deals on one simulated block of `lanes` lanes, with helping; `eager` donates whenever a
@@ -115,23 +113,21 @@ int replay_block(const uint64_t* hands, long long n, int tt_log2, int jpd, int l
     e->mask = (1u << tt_log2) - 1;
     memset(&e->st, 0, sizeof(e->st));
     e->sh = sh;
+    e->lane_id = i;
+    e->min_nodes = 0;  // donate from any job (the GPU waits for DONATE_MIN_NODES)
     envs[i] = e;
     memset(&L[i], 0, sizeof(Lane));
     L[i].stage = ST_TAKE;
     L[i].task = -1;
   }
+  sh->eager = eager != 0;
   uint64_t iters = 0;
   for (;;) {
-    int hungry = 0, busy = 0, live = 0;
-    for (int i = 0; i < lanes; i++) {
-      hungry += L[i].stage == ST_HUNGRY;
-      busy += busy_stage(L[i].stage);
-      live += L[i].stage != ST_IDLE;
-    }
+    int live = 0;
+    for (int i = 0; i < lanes; i++) live += L[i].stage != ST_IDLE;
     if (!live) break;
     if (++iters > 4000000000ull) return -2;
-    sh->busy = busy;
-    sh->budget = eager ? lanes : hungry - sh->pool.queued;
+    sh->budget = lanes;
     for (int i = 0; i < lanes; i++) {  // CHEAP (with abandoned helpers)
       if (task_abandoned(L[i], &sh->pool)) abort_task(L[i], *envs[i]);
       if (cheap_stage(L[i].stage)) advance_cheap(L[i], *envs[i]);
@@ -149,6 +145,7 @@ int replay_block(const uint64_t* hands, long long n, int tt_log2, int jpd, int l
   }
   for (int k = 0; k < MAX_TASKS; k++)
     if (sh->pool.state[k] != TASK_FREE) return -3;  // every task must be back in the pool
+  if (sh->pool.busy || sh->pool.hungry || sh->pool.queued) return -4;  // and every count at zero
   if (stats) {
     memset(stats, 0, 14 * sizeof(uint64_t));
     for (auto* e : envs) {
