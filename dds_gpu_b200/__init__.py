@@ -35,7 +35,8 @@ class _Stats(ctypes.Structure):
     _fields_ = [("nodes", ctypes.c_uint64), ("tt_probes", ctypes.c_uint64), ("tt_hits", ctypes.c_uint64),
                 ("tt_stores", ctypes.c_uint64), ("tt_bytes", ctypes.c_uint64),
                 ("enter_exit", ctypes.c_uint64 * 7), ("phase_warps", ctypes.c_uint64 * 5),
-                ("phase_items", ctypes.c_uint64 * 5), ("iterations", ctypes.c_uint64),
+                ("phase_items", ctypes.c_uint64 * 5), ("phase_cycles", ctypes.c_uint64 * 5),
+                ("iterations", ctypes.c_uint64),
                 ("tasks", ctypes.c_uint64),
                 ("jobs_done", ctypes.c_int64),
                 ("kernel_ms", ctypes.c_double), ("lanes", ctypes.c_int), ("grid", ctypes.c_int),

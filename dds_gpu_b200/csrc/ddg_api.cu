@@ -323,6 +323,7 @@ int ddg_solve_device(ddg_solver* s, const uint64_t* d_hands, int64_t n, const in
     for (int k = 0; k < PH_COUNT; k++) {
       st->phase_warps[k] = c[CNT_PHASE_WARPS + k];
       st->phase_items[k] = c[CNT_PHASE_ITEMS + k];
+      st->phase_cycles[k] = c[CNT_PHASE_CYCLES + k];
     }
     st->iterations = c[CNT_ITERS];
     st->tasks = 0;

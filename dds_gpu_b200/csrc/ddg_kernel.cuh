@@ -33,7 +33,8 @@ enum {
   CNT_JOBS_DONE = 29,
   CNT_ITERS = 30,         // block iterations
   CNT_TASKS = 31,         // tasks donated to helpers
-  CNT_WORDS = 32
+  CNT_PHASE_CYCLES = 32,  // 8 words: SM cycles per phase, summed over blocks
+  CNT_WORDS = 40
 };
 
 struct BatchArgs {
@@ -138,7 +139,10 @@ struct BlockShared {
   unsigned mask[BLOCK / 32];
   unsigned long long ph_warps[PH_COUNT], ph_items[PH_COUNT], iters;
   int stop;
-  int help_hint;  // hungry lanes outnumber queued tasks (read once per iteration)
+  int help_hint;    // hungry lanes outnumber queued tasks (read once per iteration)
+  int claim_slots;  // hungry lanes of this block that may look for a task this iteration
+  int all_done;     // no job left anywhere and no lane busy: hungry lanes stop
+  unsigned long long ph_cycles[PH_COUNT];
 };
 
 // Position of the r-th (0-based) set bit of m (r < popc(m)).
@@ -175,7 +179,9 @@ __device__ __forceinline__ void run_phase(BlockShared<BLOCK>& sh, long long base
   const int wid = tid >> 5, ln = tid & 31;
   const Lane& me = sh.lane[tid];
   bool want;
-  if (PH == PH_CHEAP) want = cheap_stage(me.stage) || (sh.args.tasks && task_abandoned(me, sh.args.tasks));
+  if (PH == PH_CHEAP)  // hungry lanes only when a task may be waiting (or to stop them)
+    want = (cheap_stage(me.stage) && (me.stage != ST_HUNGRY || sh.claim_slots > 0 || sh.all_done)) ||
+           (sh.args.tasks && task_abandoned(me, sh.args.tasks));
   else if (PH == PH_LEAD) want = me.stage == ST_ENTER && me.p.nplayed == 0;
   else if (PH == PH_FOLLOW) want = me.stage == ST_ENTER && me.p.nplayed != 0;
   else if (PH == PH_MOVES_LEAD) want = me.stage == ST_MOVES_LEAD;
@@ -200,7 +206,18 @@ __device__ __forceinline__ void run_phase(BlockShared<BLOCK>& sh, long long base
     Lane& L = sh.lane[item];
     if (PH == PH_CHEAP) {
       if (env.tp && task_abandoned(L, env.tp)) abort_task(L, env);
-      advance_cheap(L, env);
+      if (L.stage == ST_HUNGRY) {
+        if (sh.all_done) {
+          atomicAdd(&env.tp->hungry, -1);
+          L.stage = ST_IDLE;
+        } else if (atomicSub(&sh.claim_slots, 1) <= 0) {
+          L.stage = ST_HUNGRY;  // no claim this iteration
+        } else {
+          advance_cheap(L, env);
+        }
+      } else {
+        advance_cheap(L, env);
+      }
     } else if (PH == PH_LEAD || PH == PH_FOLLOW) {
       step_enter(L, env);
     } else {
@@ -233,12 +250,15 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(BatchArgs a) {
   if (tid < PH_COUNT) {
     sh.ph_warps[tid] = 0;
     sh.ph_items[tid] = 0;
+    sh.ph_cycles[tid] = 0;
   }
   if (tid == 0) {
     sh.args = a;
     sh.stop = 0;
     sh.iters = 0;
     sh.help_hint = 0;
+    sh.claim_slots = 0;
+    sh.all_done = 0;
   }
   __syncthreads();
   for (unsigned iter = 0;; iter++) {
@@ -250,13 +270,31 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(BatchArgs a) {
     }
     if (tid == 0) {
       sh.iters++;
-      if (a.tasks) sh.help_hint = atom_load(&a.tasks->hungry) > atom_load(&a.tasks->queued);
+      if (a.tasks) {  // one read of the helping counters per block and iteration
+        const int q = atom_load(&a.tasks->queued), h = atom_load(&a.tasks->hungry);
+        sh.help_hint = h > q;
+        sh.claim_slots = q > 32 ? 32 : q;
+        sh.all_done = atom_load(&a.tasks->exhausted) && atom_load(&a.tasks->busy) == 0;
+      }
     }
+    long long t0 = clock64();
     run_phase<BLOCK, PH_CHEAP>(sh, base, tid);
+    long long t1 = clock64();
     run_phase<BLOCK, PH_LEAD>(sh, base, tid);
+    long long t2 = clock64();
     run_phase<BLOCK, PH_FOLLOW>(sh, base, tid);
+    long long t3 = clock64();
     run_phase<BLOCK, PH_MOVES_LEAD>(sh, base, tid);
+    long long t4 = clock64();
     run_phase<BLOCK, PH_MOVES_FOLLOW>(sh, base, tid);
+    if (tid == 0) {
+      long long t5 = clock64();
+      sh.ph_cycles[PH_CHEAP] += t1 - t0;
+      sh.ph_cycles[PH_LEAD] += t2 - t1;
+      sh.ph_cycles[PH_FOLLOW] += t3 - t2;
+      sh.ph_cycles[PH_MOVES_LEAD] += t4 - t3;
+      sh.ph_cycles[PH_MOVES_FOLLOW] += t5 - t4;
+    }
   }
   a.lane_gen[base + tid] = sh.lane[tid].gen;
   __syncthreads();
@@ -279,6 +317,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(BatchArgs a) {
     if (tid >= CNT_PHASE_WARPS && tid < CNT_PHASE_WARPS + PH_COUNT) sum = sh.ph_warps[tid - CNT_PHASE_WARPS];
     if (tid >= CNT_PHASE_ITEMS && tid < CNT_PHASE_ITEMS + PH_COUNT) sum = sh.ph_items[tid - CNT_PHASE_ITEMS];
     if (tid == CNT_ITERS) sum = sh.iters;
+    if (tid >= CNT_PHASE_CYCLES && tid < CNT_PHASE_CYCLES + PH_COUNT) sum = sh.ph_cycles[tid - CNT_PHASE_CYCLES];
     if (tid != CNT_NEXT_JOB && sum) atomicAdd(a.counters + tid, sum);
   }
 }

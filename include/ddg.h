@@ -65,6 +65,7 @@ typedef struct ddg_stats {
                               a trick start, ENTER inside a trick, lead moves, follow moves */
   uint64_t phase_items[5]; /* lanes served by those passes; items / (32 * warps) is the
                               phase's warp efficiency */
+  uint64_t phase_cycles[5]; /* SM clock cycles spent in each phase, summed over blocks */
   uint64_t iterations;     /* block iterations, summed over blocks */
   uint64_t tasks;          /* sibling-move tasks handed to helping lanes */
   int64_t jobs_done;       /* finished jobs */
