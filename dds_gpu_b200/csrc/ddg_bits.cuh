@@ -62,6 +62,22 @@ DDG_HD int low_bit32(u32 x) {
 #endif
 }
 
+// Asks for a line to be brought into L1 (GPU) ahead of a dependent load; no-op on the host.
+DDG_HD void prefetch_l1(const void* p) {
+#ifdef __CUDA_ARCH__
+  asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+#else
+  (void)p;
+#endif
+}
+DDG_HD void prefetch_l2(const void* p) {
+#ifdef __CUDA_ARCH__
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+#else
+  (void)p;
+#endif
+}
+
 DDG_HD u64 card_bit(int c) { return (u64)1 << c; }
 DDG_HD u64 suit_cards(int s) { return (u64)0x1FFF << (16 * s); }
 DDG_HD int card_suit(int c) { return c >> 4; }

@@ -436,9 +436,23 @@ DDG_HD int task_post(TaskPool& tp, const Task& t, int start) {
 // Takes a queued task from a window of the pool starting at `start`; its id, or -1.
 DDG_HD int task_claim(TaskPool& tp, int start) {
   if (atom_load(&tp.queued) <= 0) return -1;
-  for (int j = 0; j < CLAIM_WINDOW; j++) {
-    const int k = (start + j) & (MAX_TASKS - 1);
-    if (atom_load(&tp.state[k]) == TASK_QUEUED && atom_cas(&tp.state[k], TASK_QUEUED, TASK_RUNNING) == TASK_QUEUED) {
+  start &= (MAX_TASKS - 1) & ~(CLAIM_WINDOW - 1);  // a window-aligned block of the pool
+  u64 queued = 0;  // bit j: slot start + j looked queued
+#ifdef __CUDA_ARCH__
+  // One pass of vector loads (all in flight at once) from L2, where the atomics live.
+  const int4* w = reinterpret_cast<const int4*>(tp.state + start);
+#pragma unroll
+  for (int j = 0; j < CLAIM_WINDOW / 4; j++) {
+    const int4 v = __ldcg(w + j);
+    queued |= (u64)(v.x == TASK_QUEUED) << (4 * j) | (u64)(v.y == TASK_QUEUED) << (4 * j + 1) |
+              (u64)(v.z == TASK_QUEUED) << (4 * j + 2) | (u64)(v.w == TASK_QUEUED) << (4 * j + 3);
+  }
+#else
+  for (int j = 0; j < CLAIM_WINDOW; j++) queued |= (u64)(tp.state[start + j] == TASK_QUEUED) << j;
+#endif
+  for (; queued; queued &= queued - 1) {
+    const int k = start + low_bit(queued);
+    if (atom_cas(&tp.state[k], TASK_QUEUED, TASK_RUNNING) == TASK_QUEUED) {
       atom_add(&tp.queued, -1);
       fence_block();
       return k;
@@ -501,12 +515,14 @@ enum { PH_FIRST = 0, PH_UP = 1, PH_DOWN = 2 };
 // A lane's whole state between stages (192 bytes; in shared memory on the GPU).
 struct Lane {
   Pos p;
-  Frame f;  // top of the stack
-  Top top;  // trick-start table of an expanding lead node (ENTER -> MOVES_LEAD)
+  Frame f;    // top of the stack
+  Frame par;  // copy of the frame last pushed to the stack (depth par_sp): most pops need no load
+  Top top;    // trick-start table of an expanding lead node (ENTER -> MOVES_LEAD)
   u64 r;    // relevant cards of the node just finished
   long long job, deal;
   u32 gen;
   int16_t task;      // the task this lane helps with, or -1 (its own job)
+  int8_t par_sp;     // depth of `par`, or -1
   int8_t stage, sp;  // sp = depth of f; frames 0..sp-1 are in the lane's stack
   int8_t target;     // the null-window search in progress: NS >= target?
   int8_t lo, hi;     // MODE_BISECT: answer in [lo, hi]; MODE_STEP: lo = t, hi = phase
@@ -522,6 +538,7 @@ DDG_HD void start_search(Lane& L) {
   L.p.left = popc(L.p.h[0]);
   L.p.trick = 0;
   L.sp = 0;
+  L.par_sp = -1;
   L.stage = ST_ENTER;
 }
 
@@ -606,7 +623,14 @@ template <class Env>
 DDG_HD void node_done(Lane& L, Env& env) {
   if (L.sp > 0) {
     L.sp--;
-    frame_load(L.f, env.stack + L.sp);
+    if (L.par_sp == L.sp) L.f = L.par;  // the frame pushed last: still in shared memory
+    else frame_load(L.f, env.stack + L.sp);
+    L.par_sp = -1;
+    if (L.sp > 0) {  // the next pop's frame, on its way to L1
+      const char* g = reinterpret_cast<const char*>(env.stack + L.sp - 1);
+      prefetch_l1(g);
+      prefetch_l1(g + sizeof(Frame) - 1);
+    }
     L.stage = ST_RET;
     return;
   }
@@ -667,6 +691,7 @@ DDG_HD void step_root(Lane& L, Env& env) {
   if (L.target >= 0) return;
   // Answered without a search (a seed of 0 with no tricks left).
   L.sp = 0;
+  L.par_sp = -1;
   L.v = 1;
   int ans = L.lo;
   for (;;) {
@@ -745,7 +770,11 @@ DDG_HD void step_next(Lane& L, Env& env) {
       f.tried |= card_bit(card);
       play(L.p, f, card);
       frame_store(env.stack + L.sp, f);
+      L.par = f;
+      L.par_sp = L.sp;
       L.sp++;
+      if (L.p.nplayed == 0)  // a trick start next: its TT tag line, on its way to L2
+        prefetch_l2(env.tt + (key_hash(length_key(L.p.h), L.p.leader) & env.mask));
       L.stage = ST_ENTER;
       return;
     }
@@ -835,6 +864,7 @@ DDG_HD bool step_hungry(Lane& L, Env& env) {
   L.f.info = k.info;
   L.f.pad = 0;
   L.sp = 0;
+  L.par_sp = -1;
   L.target = k.target;
   L.task = (int16_t)t;
   L.gen = tt_next_gen(env.tt, env.mask, L.gen);
@@ -871,6 +901,7 @@ DDG_HD bool task_abandoned(const Lane& L, const TaskPool* tp) {
 template <class Env>
 DDG_HD bool try_donate(Lane& L, Env& env) {
   const int top = L.sp < MAX_DONATE_DEPTH ? L.sp : MAX_DONATE_DEPTH;
+  for (int d = 0; d < top; d++) prefetch_l1(env.stack + d);  // the scan's loads, in flight together
   for (int d = 0; d < top; d++) {
     Frame g;
     frame_load(g, env.stack + d);
@@ -905,6 +936,7 @@ DDG_HD bool try_donate(Lane& L, Env& env) {
     fr_set_task(g, id, n);
     fr_set_n(g, i + 1);
     frame_store(env.stack + d, g);
+    if (L.par_sp == d) L.par = g;
     return true;
   }
   return false;
