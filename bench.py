@@ -42,11 +42,14 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--batch", type=int, default=2048, help="deals per step per GPU")
+    p.add_argument("--batch", type=int, default=1024, help="deals per step per GPU")
     p.add_argument("--tt-log2", type=int, default=10)
     p.add_argument("--lanes", type=int, default=0, help="0 = fill the GPU")
     p.add_argument("--jpd", type=int, default=20, help="jobs per deal: 5 (per strain) or 20 (per lead)")
-    p.add_argument("--block", type=int, default=128)
+    p.add_argument("--block", type=int, default=256)
+    p.add_argument("--min-blocks", type=int, default=2)
+    p.add_argument("--help-lanes", type=int, default=1, help="1: idle lanes help busy ones (same tricks)")
+    p.add_argument("--safety-s", type=float, default=900.0, help="per-step stop; a stopped step is an error")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-deals", type=int, default=0, help="deals per CPU sample (0 = one per core)")
@@ -205,7 +208,8 @@ def our_arm(a, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     deals = ddg.make_deals(SET_SEED, 0, SET_SIZE, SET_K)
-    solver = ddg.Solver(tt_log2=a.tt_log2, lanes=a.lanes, block=a.block, jobs_per_deal=a.jpd, device=local_rank)
+    solver = ddg.Solver(tt_log2=a.tt_log2, lanes=a.lanes, block=a.block, jobs_per_deal=a.jpd, device=local_rank,
+                        min_blocks=a.min_blocks, help=a.help_lanes, time_limit_s=a.safety_s)
     B = a.batch
     nsteps = a.warmup + a.steps
 
@@ -216,7 +220,8 @@ def our_arm(a, rank, world, local_rank):
     host_in = [torch.from_numpy(np.ascontiguousarray(deals[step_idx(s)]).view(np.int64)).pin_memory()
                for s in range(nsteps)]
     dev_in = [h.to(dev) for h in host_in]
-    dev_out = torch.empty((B, 20), dtype=torch.uint8, device=dev)
+    dev_outs = [torch.empty((B, 20), dtype=torch.uint8, device=dev) for _ in range(nsteps)]
+    dev_out = dev_outs[0]
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream(dev)
 
@@ -239,13 +244,15 @@ def our_arm(a, rank, world, local_rank):
     e0.record(stream)
     for s in range(a.warmup, nsteps):
         flush.zero_()
-        stats.append(solver.solve_device(dev_in[s].data_ptr(), B, dev_out.data_ptr(), stream=stream.cuda_stream))
+        stats.append(solver.solve_device(dev_in[s].data_ptr(), B, dev_outs[s].data_ptr(), stream=stream.cuda_stream))
     e1.record(stream)
     torch.cuda.synchronize(dev)
     barrier()
     clocks = sampler.stop()
     elapsed_ms = e0.elapsed_time(e1)
-    unsolved = int((dev_out == 255).sum().item())
+    # Every result of every timed step must be there (the safety stop leaves 255s).
+    unsolved = sum(int((dev_outs[s] == 255).sum().item()) for s in range(a.warmup, nsteps))
+    tables = [dev_outs[s].cpu().numpy() for s in range(a.warmup, nsteps)]
 
     # End to end through the host API: pinned deals in, results out, every step.
     e2e_ms = None
@@ -279,8 +286,9 @@ def our_arm(a, rank, world, local_rank):
     kernel_ms = sum(s["kernel_ms"] for s in stats)
     nodes = sum(s["nodes"] for s in stats)
     tt_bytes = sum(s["tt_bytes"] for s in stats)
-    it = [sum(s["stage_iters"][k] for s in stats) for k in range(6)]
-    ln = [sum(s["stage_lanes"][k] for s in stats) for k in range(6)]
+    it = [sum(s["phase_warps"][k] for s in stats) for k in range(5)]
+    ln = [sum(s["phase_items"][k] for s in stats) for k in range(5)]
+    tasks = sum(s["tasks"] for s in stats)
     if world > 1:
         t = torch.tensor([nodes, tt_bytes], dtype=torch.float64, device=dev)
         torch.distributed.all_reduce(t)
@@ -308,7 +316,7 @@ def our_arm(a, rank, world, local_rank):
     deals_total = a.steps * B * world
     value = deals_total / (elapsed_ms * 1e-3)
     eff = {name: (ln[k] / (32.0 * it[k]) if it[k] else None)
-           for k, name in enumerate(["take", "root", "enter", "next", "ret"])}
+           for k, name in enumerate(["cheap", "enter_lead", "enter_follow", "moves_lead", "moves_follow"])}
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tfile):
@@ -326,6 +334,7 @@ def our_arm(a, rank, world, local_rank):
                                          "block": a.block, "guide": "off (plain DDS move order)"}),
         "nodes_per_deal": nodes_all / deals_total, "nodes_per_s": nodes_all / (elapsed_ms * 1e-3),
         "unsolved_results": unsolved,
+        "helping_tasks": tasks,
         "warp_efficiency": eff,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
