@@ -28,7 +28,8 @@ class _Config(ctypes.Structure):
     _fields_ = [("tt_log2", ctypes.c_int), ("lanes", ctypes.c_int), ("block", ctypes.c_int),
                 ("jobs_per_deal", ctypes.c_int), ("device", ctypes.c_int), ("schedule", ctypes.c_int),
                 ("min_blocks", ctypes.c_int), ("time_limit_s", ctypes.c_double),
-                ("mem_fraction", ctypes.c_double), ("help", ctypes.c_int)]
+                ("mem_fraction", ctypes.c_double), ("help", ctypes.c_int), ("free_below", ctypes.c_int),
+                ("free_steps", ctypes.c_int)]
 
 
 class _Stats(ctypes.Structure):
@@ -36,6 +37,7 @@ class _Stats(ctypes.Structure):
                 ("tt_stores", ctypes.c_uint64), ("tt_bytes", ctypes.c_uint64),
                 ("enter_exit", ctypes.c_uint64 * 7), ("phase_warps", ctypes.c_uint64 * 5),
                 ("phase_items", ctypes.c_uint64 * 5), ("phase_cycles", ctypes.c_uint64 * 5),
+                ("free_rounds", ctypes.c_uint64), ("free_cycles", ctypes.c_uint64),
                 ("iterations", ctypes.c_uint64),
                 ("tasks", ctypes.c_uint64),
                 ("jobs_done", ctypes.c_int64),
@@ -109,7 +111,7 @@ class Solver:
     """A solver pool on one GPU (ddg_solver_create): per-lane TTs and stacks in HBM."""
 
     def __init__(self, tt_log2=10, lanes=0, block=128, jobs_per_deal=5, device=0, schedule=0,
-                 time_limit_s=0.0, mem_fraction=0.85, min_blocks=0, help=0):
+                 time_limit_s=0.0, mem_fraction=0.85, min_blocks=0, help=0, free_below=0, free_steps=0):
         lib = load_library()
         cfg = _Config()
         lib.ddg_config_default(ctypes.byref(cfg))
@@ -117,6 +119,7 @@ class Solver:
         cfg.jobs_per_deal, cfg.device, cfg.schedule = jobs_per_deal, device, schedule
         cfg.min_blocks = min_blocks
         cfg.help = help
+        cfg.free_below, cfg.free_steps = free_below, free_steps
         cfg.time_limit_s, cfg.mem_fraction = time_limit_s, mem_fraction
         self._lib = lib
         self._h = P()

@@ -290,6 +290,8 @@ int ddg_solve_device(ddg_solver* s, const uint64_t* d_hands, int64_t n, const in
   a.stop = s->d_stop;
   a.job_end_ns = s->d_job_end_ns;
   a.tasks = s->tasks;
+  a.free_below = s->cfg.free_below == 0 ? 64 : s->cfg.free_below < 0 ? 0 : s->cfg.free_below;
+  a.free_steps = s->cfg.free_steps > 0 ? s->cfg.free_steps : 256;
   if (s->tasks) CUDA_TRY(cudaMemsetAsync(s->tasks, 0, sizeof(TaskPool), stream));
   if (s->d_job_end_ns) CUDA_TRY(cudaMemsetAsync(s->d_job_end_ns, 0, (size_t)n_jobs * 8, stream));
   CUDA_TRY(cudaEventRecord(s->ev0, stream));
@@ -325,6 +327,8 @@ int ddg_solve_device(ddg_solver* s, const uint64_t* d_hands, int64_t n, const in
       st->phase_items[k] = c[CNT_PHASE_ITEMS + k];
       st->phase_cycles[k] = c[CNT_PHASE_CYCLES + k];
     }
+    st->free_rounds = c[CNT_PHASE_ITEMS + PH_COUNT];
+    st->free_cycles = c[CNT_PHASE_CYCLES + PH_COUNT];
     st->iterations = c[CNT_ITERS];
     st->tasks = 0;
     if (s->tasks) {

@@ -54,6 +54,8 @@ struct BatchArgs {
   volatile int* stop;    // host-set stop flag (mapped memory), or null
   u64* job_end_ns;       // n * jpd completion times (device global timer, ns), or null
   TaskPool* tasks;       // helping: idle lanes take donated moves (tricks exact), or null
+  int free_below;        // fewer busy lanes than this in a block: each thread runs its own lane
+  int free_steps;        // stages a lane runs per free-running round
 };
 
 __device__ __forceinline__ u64 global_ns() {
@@ -143,6 +145,7 @@ struct BlockShared {
   int claim_slots;  // hungry lanes of this block that may look for a task this iteration
   int all_done;     // no job left anywhere and no lane busy: hungry lanes stop
   unsigned long long ph_cycles[PH_COUNT];
+  unsigned long long free_rounds, free_cycles;  // free-running rounds and their SM cycles
 };
 
 // Position of the r-th (0-based) set bit of m (r < popc(m)).
@@ -259,6 +262,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(BatchArgs a) {
     sh.help_hint = 0;
     sh.claim_slots = 0;
     sh.all_done = 0;
+    sh.free_rounds = 0;
+    sh.free_cycles = 0;
   }
   __syncthreads();
   for (unsigned iter = 0;; iter++) {
@@ -276,6 +281,28 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(BatchArgs a) {
         sh.claim_slots = q > 32 ? 32 : q;
         sh.all_done = atom_load(&a.tasks->exhausted) && atom_load(&a.tasks->busy) == 0;
       }
+    }
+    const int st0 = sh.lane[tid].stage;
+    const int busy_here = __syncthreads_count(st0 != ST_HUNGRY && st0 != ST_IDLE);
+    if (busy_here < a.free_below) {
+      // Few busy lanes: each thread runs its own lane for a while, no phases.
+      const long long f0 = clock64();
+      Lane& L = sh.lane[tid];
+      if (L.stage == ST_HUNGRY && sh.all_done) {
+        atomicAdd(&a.tasks->hungry, -1);
+        L.stage = ST_IDLE;
+      } else if (L.stage != ST_IDLE) {
+        DevEnv env = lane_env(sh, base + tid, tid);
+        if (env.tp && task_abandoned(L, env.tp)) abort_task(L, env);
+        const bool may_claim = L.stage == ST_HUNGRY && atomicSub(&sh.claim_slots, 1) > 0;
+        advance_free(L, env, a.free_steps, may_claim);
+      }
+      __syncthreads();
+      if (tid == 0) {
+        sh.free_rounds++;
+        sh.free_cycles += clock64() - f0;
+      }
+      continue;
     }
     long long t0 = clock64();
     run_phase<BLOCK, PH_CHEAP>(sh, base, tid);
@@ -318,6 +345,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(BatchArgs a) {
     if (tid >= CNT_PHASE_ITEMS && tid < CNT_PHASE_ITEMS + PH_COUNT) sum = sh.ph_items[tid - CNT_PHASE_ITEMS];
     if (tid == CNT_ITERS) sum = sh.iters;
     if (tid >= CNT_PHASE_CYCLES && tid < CNT_PHASE_CYCLES + PH_COUNT) sum = sh.ph_cycles[tid - CNT_PHASE_CYCLES];
+    if (tid == CNT_PHASE_CYCLES + PH_COUNT) sum = sh.free_cycles;
+    if (tid == CNT_PHASE_ITEMS + PH_COUNT) sum = sh.free_rounds;
     if (tid != CNT_NEXT_JOB && sum) atomicAdd(a.counters + tid, sum);
   }
 }

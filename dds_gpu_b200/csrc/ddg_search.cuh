@@ -974,6 +974,41 @@ DDG_HD void advance_cheap(Lane& L, Env& env) {
   }
 }
 
+// Up to `max_steps` stages of one lane, whatever they are: the free-running mode of a block
+// with few busy lanes (each thread then runs its own lane without waiting for the others).
+// A hungry lane looks for a task only when `may_claim`; a waiting lane stops until its
+// helper is done.
+template <class Env>
+DDG_HD void advance_free(Lane& L, Env& env, int max_steps, bool may_claim) {
+  bool offered = false;
+  for (int k = 0; k < max_steps; k++) {
+    switch (L.stage) {
+      case ST_IDLE: return;
+      case ST_HUNGRY:
+        if (!may_claim || !step_hungry(L, env)) return;
+        may_claim = false;
+        break;
+      case ST_WAIT:
+        if (!step_wait(L, env)) return;
+        break;
+      case ST_NEXT:
+        if (!offered && env.pool() && L.sp > 0 && env.work_nodes() >= DONATE_MIN_NODES && env.want_donation()) {
+          offered = true;
+          if (!try_donate(L, env)) env.unreserve();
+        }
+        step_next(L, env);
+        break;
+      case ST_TAKE: step_take(L, env); break;
+      case ST_ROOT: step_root(L, env); break;
+      case ST_ENTER: step_enter(L, env); break;
+      case ST_MOVES_LEAD:
+      case ST_MOVES_FOLLOW: step_moves(L, env); break;
+      case ST_RET: step_ret(L, env); break;
+      default: return;
+    }
+  }
+}
+
 // One stage of the lane, whatever it is (the host replay steps lanes this way).
 template <class Env>
 DDG_HD void lane_step(Lane& L, Env& env) {

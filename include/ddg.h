@@ -50,6 +50,9 @@ typedef struct ddg_config {
   int help;             /* 1: once the job queue is empty, idle lanes take over untried sibling
                            moves of busy lanes in their block (same tricks, other node counts);
                            0: every job is searched by one lane, nodes equal the reference's */
+  int free_below;       /* a block with fewer busy lanes than this runs each lane on its own
+                           thread (no phases): faster lanes in the batch's tail. 0 = 64, -1 = never */
+  int free_steps;       /* stages per lane per free-running round; 0 = 256 */
 } ddg_config;
 
 /* Counters of one solve call (device-side counters, summed over lanes). */
@@ -66,6 +69,8 @@ typedef struct ddg_stats {
   uint64_t phase_items[5]; /* lanes served by those passes; items / (32 * warps) is the
                               phase's warp efficiency */
   uint64_t phase_cycles[5]; /* SM clock cycles spent in each phase, summed over blocks */
+  uint64_t free_rounds;    /* free-running rounds (blocks with few busy lanes), summed over blocks */
+  uint64_t free_cycles;    /* SM clock cycles of those rounds */
   uint64_t iterations;     /* block iterations, summed over blocks */
   uint64_t tasks;          /* sibling-move tasks handed to helping lanes */
   int64_t jobs_done;       /* finished jobs */

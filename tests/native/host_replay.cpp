@@ -88,8 +88,8 @@ extern "C" {
 // n deals on one simulated block of `lanes` lanes, with helping; `eager` donates whenever a
 // lane could (not only when lanes are hungry). Results and nodes as replay_solve; stats[12]
 // = tasks posted, stats[13] = block iterations.
-int replay_block(const uint64_t* hands, long long n, int tt_log2, int jpd, int lanes, int eager, int* out20,
-                 uint64_t* stats) {
+int replay_block(const uint64_t* hands, long long n, int tt_log2, int jpd, int lanes, int eager, int free_below,
+                 int free_steps, int* out20, uint64_t* stats) {
   if (tt_log2 < TT_MIN_LOG2 || tt_log2 > 16 || (jpd != 5 && jpd != 20) || lanes < 1 || lanes > 1024) return -1;
   std::atomic<long long> next{0};
   SimShared* sh = new SimShared();
@@ -128,6 +128,21 @@ int replay_block(const uint64_t* hands, long long n, int tt_log2, int jpd, int l
     if (!live) break;
     if (++iters > 4000000000ull) return -2;
     sh->budget = lanes;
+    int busy = 0;
+    for (int i = 0; i < lanes; i++) busy += L[i].stage != ST_HUNGRY && L[i].stage != ST_IDLE;
+    if (busy < free_below) {  // the kernel's free-running round, lane by lane
+      const bool all_done = sh->pool.exhausted && sh->pool.busy == 0;
+      for (int i = 0; i < lanes; i++) {
+        if (L[i].stage == ST_HUNGRY && all_done) {
+          sh->pool.hungry--;
+          L[i].stage = ST_IDLE;
+          continue;
+        }
+        if (task_abandoned(L[i], &sh->pool)) abort_task(L[i], *envs[i]);
+        advance_free(L[i], *envs[i], free_steps, L[i].stage == ST_HUNGRY);
+      }
+      continue;
+    }
     for (int i = 0; i < lanes; i++) {  // CHEAP (with abandoned helpers)
       if (task_abandoned(L[i], &sh->pool)) abort_task(L[i], *envs[i]);
       if (cheap_stage(L[i].stage)) advance_cheap(L[i], *envs[i]);

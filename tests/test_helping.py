@@ -12,21 +12,22 @@ from conftest import load_golden
 P = ctypes.c_void_p
 
 
-def block(lib, hands, lanes, eager, jpd=5, tt_log2=10):
+def block(lib, hands, lanes, eager, jpd=5, tt_log2=10, free_below=0, free_steps=64):
     n = hands.shape[0]
     h = np.ascontiguousarray(hands, dtype=np.uint64)
     out = np.zeros(n * 20, np.int32)
     st = np.zeros(14, np.uint64)
-    rc = lib.replay_block(h.ctypes.data_as(P), ctypes.c_longlong(n), tt_log2, jpd, lanes, eager,
-                          out.ctypes.data_as(P), st.ctypes.data_as(P))
+    rc = lib.replay_block(h.ctypes.data_as(P), ctypes.c_longlong(n), tt_log2, jpd, lanes, eager, free_below,
+                          free_steps, out.ctypes.data_as(P), st.ctypes.data_as(P))
     return rc, out.reshape(n, 5, 4), st
 
 
 @pytest.mark.parametrize("name", ["k4_120.npz", "k6_120.npz", "k8_120.npz", "k9_120.npz"])
-@pytest.mark.parametrize("lanes,eager,jpd", [(3, 1, 5), (16, 0, 20), (16, 1, 20), (64, 1, 5)])
-def test_helping_keeps_tricks(replay_lib, name, lanes, eager, jpd):
+@pytest.mark.parametrize("lanes,eager,jpd,free", [(3, 1, 5, 0), (16, 0, 20, 0), (16, 1, 20, 0), (64, 1, 5, 0),
+                                                  (16, 1, 20, 8), (64, 0, 5, 40), (32, 1, 20, 1000)])
+def test_helping_keeps_tricks(replay_lib, name, lanes, eager, jpd, free):
     g = load_golden(name)
-    rc, t, st = block(replay_lib, g["hands"][:48], lanes, eager, jpd)
+    rc, t, st = block(replay_lib, g["hands"][:48], lanes, eager, jpd, free_below=free, free_steps=17)
     assert rc == 0
     assert (t == g["tricks"][:48]).all()
     if eager:
