@@ -620,7 +620,7 @@ DDG_HD int root_result(Lane& L) {
 //   TTBucket* tt; u32 mask      the lane's TT
 //   LaneStats& stats()          the lane's counters (kept out of registers on the GPU)
 template <class Env>
-DDG_HD void node_done(Lane& L, Env& env) {
+DDG_CALL void node_done(Lane& L, Env& env) {
   if (L.sp > 0) {
     L.sp--;
     if (L.par_sp == L.sp) L.f = L.par;  // the frame pushed last: still in shared memory
@@ -665,7 +665,7 @@ DDG_HD void node_done(Lane& L, Env& env) {
 //   u64 work_nodes()        nodes searched since the lane's job or task began
 
 template <class Env>
-DDG_HD void step_take(Lane& L, Env& env) {
+DDG_CALL void step_take(Lane& L, Env& env) {
   TaskPool* tp = env.pool();
   if (!env.take(L)) {
     if (tp) {
@@ -686,7 +686,7 @@ DDG_HD void step_take(Lane& L, Env& env) {
 }
 
 template <class Env>
-DDG_HD void step_root(Lane& L, Env& env) {
+DDG_CALL void step_root(Lane& L, Env& env) {
   start_lead(L, env.seed(L));
   if (L.target >= 0) return;
   // Answered without a search (a seed of 0 with no tricks left).
@@ -724,7 +724,7 @@ DDG_HD void step_enter(Lane& L, Env& env) {
 }
 
 template <class Env>
-DDG_HD void step_moves(Lane& L, Env& env) {
+DDG_CALL void step_moves(Lane& L, Env& env) {
   if (L.stage == ST_MOVES_LEAD) gen_moves_lead(L.p, frame_hint(L.f), L.top, L.f);
   else gen_moves_follow(L.p, L.f);
   L.stage = ST_NEXT;
@@ -734,7 +734,7 @@ DDG_HD void step_moves(Lane& L, Env& env) {
 // widening, no TT store: the frame holds only part of the node's moves); any other
 // frame is finished and returns to its parent.
 template <class Env>
-DDG_HD void frame_done(Lane& L, Env& env) {
+DDG_CALL void frame_done(Lane& L, Env& env) {
   Frame& f = L.f;
   if (L.sp == 0 && L.task >= 0) {
     TaskPool& tp = *env.pool();
@@ -751,7 +751,7 @@ DDG_HD void frame_done(Lane& L, Env& env) {
 
 // NEXT: play the frame's next candidate (src/dd.h:812-835), or finish the node.
 template <class Env>
-DDG_HD void step_next(Lane& L, Env& env) {
+DDG_CALL void step_next(Lane& L, Env& env) {
   Frame& f = L.f;
   for (;;) {
     int i = fr_i(f);
@@ -810,7 +810,7 @@ DDG_HD void step_next(Lane& L, Env& env) {
 
 // RET: the child of the top frame returned (L.v, L.r) (src/dd.h:840-854).
 template <class Env>
-DDG_HD void step_ret(Lane& L, Env& env) {
+DDG_CALL void step_ret(Lane& L, Env& env) {
   Frame& f = L.f;
   int card = fr_move(f, fr_i(f));
   unplay(L.p, f, card, L.r);
@@ -841,7 +841,7 @@ DDG_HD bool step_wait(Lane& L, Env& env) {
 
 // HUNGRY: take a task of the block, or stop when nothing is left to do.
 template <class Env>
-DDG_HD bool step_hungry(Lane& L, Env& env) {
+DDG_CALL bool step_hungry(Lane& L, Env& env) {
   TaskPool& tp = *env.pool();
   const int t = task_claim(tp, env.claim_start());
   if (t < 0) {
@@ -874,7 +874,7 @@ DDG_HD bool step_hungry(Lane& L, Env& env) {
 
 // A helper whose task was abandoned stops, and abandons what it had donated itself.
 template <class Env>
-DDG_HD void abort_task(Lane& L, Env& env) {
+DDG_CALL void abort_task(Lane& L, Env& env) {
   TaskPool& tp = *env.pool();
   for (int k = 0; k < L.sp; k++) {
     Frame g;
@@ -899,7 +899,7 @@ DDG_HD bool task_abandoned(const Lane& L, const TaskPool* tp) {
 // searched without a cutoff. The lane is in NEXT, so its position is that of the top
 // frame; the donated frame's position is found by taking back the moves above it.
 template <class Env>
-DDG_HD bool try_donate(Lane& L, Env& env) {
+DDG_CALL bool try_donate(Lane& L, Env& env) {
   const int top = L.sp < MAX_DONATE_DEPTH ? L.sp : MAX_DONATE_DEPTH;
   for (int d = 0; d < top; d++) prefetch_l1(env.stack + d);  // the scan's loads, in flight together
   for (int d = 0; d < top; d++) {
@@ -949,7 +949,7 @@ DDG_HD bool cheap_stage(int st) {
 // Runs the cheap stages back to back until the lane needs ENTER, waits, or has nothing
 // left. A lane about to play its next move first donates when its block is hungry.
 template <class Env>
-DDG_HD void advance_cheap(Lane& L, Env& env) {
+DDG_CALL void advance_cheap(Lane& L, Env& env) {
   bool offered = false;
   for (;;) {
     switch (L.stage) {
@@ -979,7 +979,7 @@ DDG_HD void advance_cheap(Lane& L, Env& env) {
 // A hungry lane looks for a task only when `may_claim`; a waiting lane stops until its
 // helper is done.
 template <class Env>
-DDG_HD void advance_free(Lane& L, Env& env, int max_steps, bool may_claim) {
+DDG_CALL void advance_free(Lane& L, Env& env, int max_steps, bool may_claim) {
   bool offered = false;
   for (int k = 0; k < max_steps; k++) {
     switch (L.stage) {

@@ -16,3 +16,11 @@ g++ -O3 -std=c++17 -march=x86-64-v3 -pthread -fPIC -shared -I"$REF_DIR/src" \
   -o "$OUT/libddref.so.tmp" "$HERE/ref_shim.cpp"
 mv "$OUT/libddref.so.tmp" "$OUT/libddref.so"
 echo "built $OUT/libddref.so"
+# The reference's own GPU batch driver (gpu/gpu_main.cu), for sm_100a: a timing baseline
+# of its wavefront kernel on the same GPU (run with WAVE=1 and CHECK=0).
+if command -v nvcc > /dev/null && [ -f "$REF_DIR/gpu/gpu_main.cu" ]; then
+  nvcc -O3 -std=c++17 -gencode arch=compute_100a,code=sm_100a -I"$REF_DIR/src" \
+    -o "$OUT/dd_gpu_ref.tmp" "$REF_DIR/gpu/gpu_main.cu"
+  mv "$OUT/dd_gpu_ref.tmp" "$OUT/dd_gpu_ref"
+  echo "built $OUT/dd_gpu_ref"
+fi
