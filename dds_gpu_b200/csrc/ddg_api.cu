@@ -97,21 +97,26 @@ int ddg_check_deal(const uint64_t* h) {
 // allocator is held to (1 = no limit beyond the block size).
 typedef void (*BatchFn)(BatchArgs);
 struct KVariant {
-  int block, minb;
+  int block, minb, schedule;
   BatchFn fn;
   size_t smem;  // dynamic shared memory per block
 };
-#define DDG_VARIANT(B, M) {B, M, batch_kernel<B, M>, sizeof(BlockShared<B>)}
+// schedule 0: block-phase kernel (all warps run each phase in turn); schedule 1: queue
+// kernel (warps take lanes from per-phase queues, no block barriers).
+#define DDG_VARIANT(B, M)                                     \
+  {B, M, 0, batch_kernel<B, M>, sizeof(BlockShared<B>)}, { \
+    B, M, 1, queue_kernel<B, M>, sizeof(BlockShared<B>)    \
+  }
 static const KVariant kVariants[] = {
-    DDG_VARIANT(64, 1),  DDG_VARIANT(128, 1), DDG_VARIANT(128, 4), DDG_VARIANT(128, 6), DDG_VARIANT(128, 8),
-    DDG_VARIANT(256, 1), DDG_VARIANT(256, 2), DDG_VARIANT(256, 3), DDG_VARIANT(256, 4),
+    DDG_VARIANT(64, 1),  DDG_VARIANT(128, 1), DDG_VARIANT(128, 4), DDG_VARIANT(128, 6),
+    DDG_VARIANT(256, 1), DDG_VARIANT(256, 2), DDG_VARIANT(256, 3),
 };
 #undef DDG_VARIANT
 
-static const KVariant* find_variant(int block, int minb) {
+static const KVariant* find_variant(int block, int minb, int schedule) {
   if (minb <= 0) minb = 1;
   for (const KVariant& v : kVariants)
-    if (v.block == block && v.minb == minb) return &v;
+    if (v.block == block && v.minb == minb && v.schedule == schedule) return &v;
   return nullptr;
 }
 
@@ -153,9 +158,10 @@ int ddg_solver_create(const ddg_config* cfg_in, ddg_solver** out) {
   }
   if (cfg.tt_log2 < TT_MIN_LOG2 || cfg.tt_log2 > 20)
     return fail(DDG_E_ARG, "tt_log2 %d is not in 9..20", cfg.tt_log2);
-  const KVariant* variant = find_variant(cfg.block, cfg.min_blocks);
+  if (cfg.schedule != 0 && cfg.schedule != 1) return fail(DDG_E_ARG, "schedule %d is not 0 or 1", cfg.schedule);
+  const KVariant* variant = find_variant(cfg.block, cfg.min_blocks, cfg.schedule);
   if (!variant)
-    return fail(DDG_E_ARG, "no kernel for block %d / min_blocks %d (64/1, 128/1,4,6,8, 256/1..4)", cfg.block,
+    return fail(DDG_E_ARG, "no kernel for block %d / min_blocks %d (64/1, 128/1,4,6, 256/1..3)", cfg.block,
                 cfg.min_blocks);
   if (cfg.jobs_per_deal != 5 && cfg.jobs_per_deal != 20)
     return fail(DDG_E_ARG, "jobs_per_deal %d is not 5 or 20", cfg.jobs_per_deal);
@@ -315,6 +321,8 @@ int ddg_solve_device(ddg_solver* s, const uint64_t* d_hands, int64_t n, const in
   unsigned long long c[CNT_WORDS];
   CUDA_TRY(cudaMemcpy(c, s->counters, sizeof(c), cudaMemcpyDeviceToHost));
   s->total_nodes += c[CNT_NODES];
+  if (c[CNT_FAULTS])
+    return fail(DDG_E_TIMEOUT, "%llu blocks gave up a bounded queue wait; results incomplete", c[CNT_FAULTS]);
   if (st) {
     st->nodes = c[CNT_NODES];
     st->tt_probes = c[CNT_PROBES];

@@ -34,6 +34,7 @@ enum {
   CNT_ITERS = 30,         // block iterations
   CNT_TASKS = 31,         // tasks donated to helpers
   CNT_PHASE_CYCLES = 32,  // 8 words: SM cycles per phase, summed over blocks
+  CNT_FAULTS = 38,        // blocks whose bounded queue wait gave up (never expected)
   CNT_WORDS = 40
 };
 
@@ -67,6 +68,7 @@ __device__ __forceinline__ u64 global_ns() {
 struct LaneCounters {
   LaneStats s;
   u64 start_nodes;
+  u64 tt_key;  // (deal, strain) key of the helper tasks the lane's TT holds, 0 = none
   u32 jobs_done;
 };
 
@@ -93,6 +95,7 @@ struct DevEnv {
   __device__ __forceinline__ int claim_start() { return (int)((lane * 61) + (global_ns() >> 12)); }
   __device__ __forceinline__ u64 work_nodes() { return c->s.nodes - c->start_nodes; }
   __device__ __forceinline__ void task_started() { c->start_nodes = c->s.nodes; }
+  __device__ __forceinline__ u64& tt_key() { return c->tt_key; }
   __device__ __forceinline__ bool take(Lane& L) {
     unsigned long long job = atomicAdd(a->counters + CNT_NEXT_JOB, 1ull);
     if ((long long)job >= a->n_jobs) return false;
@@ -146,6 +149,13 @@ struct BlockShared {
   int all_done;     // no job left anywhere and no lane busy: hungry lanes stop
   unsigned long long ph_cycles[PH_COUNT];
   unsigned long long free_rounds, free_cycles;  // free-running rounds and their SM cycles
+  // Stage queues of the queue kernel: per phase a ring of lane ids + 1 (0 = slot not yet
+  // written). Every lane is in at most one ring, so a ring never holds more than BLOCK.
+  uint16_t q[PH_COUNT][BLOCK];
+  unsigned qhead[PH_COUNT], qtail[PH_COUNT];
+  unsigned parked[BLOCK / 32];  // lanes waiting on the task pool (HUNGRY, WAIT)
+  int live;                     // lanes not IDLE
+  int fault;                    // a queue slot was never written (bounded wait gave up)
 };
 
 // Position of the r-th (0-based) set bit of m (r < popc(m)).
@@ -230,6 +240,9 @@ __device__ __forceinline__ void run_phase(BlockShared<BLOCK>& sh, long long base
   }
   __syncthreads();
 }
+
+template <int BLOCK>
+__device__ __forceinline__ void block_counters(BlockShared<BLOCK>& sh, const BatchArgs& a, int tid);
 
 // BLOCK threads (= lanes) per block; MINB resident blocks per SM asked of the register
 // allocator.
@@ -325,6 +338,212 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(BatchArgs a) {
   }
   a.lane_gen[base + tid] = sh.lane[tid].gen;
   __syncthreads();
+  block_counters(sh, a, tid);
+}
+
+// Phase queue of a lane's next stage, or -1 (parked on the task pool) / -2 (idle).
+__device__ __forceinline__ int next_queue(const Lane& L) {
+  switch (L.stage) {
+    case ST_ENTER: return L.p.nplayed == 0 ? PH_LEAD : PH_FOLLOW;
+    case ST_MOVES_LEAD: return PH_MOVES_LEAD;
+    case ST_MOVES_FOLLOW: return PH_MOVES_FOLLOW;
+    case ST_HUNGRY:
+    case ST_WAIT: return -1;
+    case ST_IDLE: return -2;
+    default: return PH_CHEAP;
+  }
+}
+
+// Hands lane `lane` (held by this thread) to the queue of its next stage. All threads of
+// the warp call this; `active` says whether this thread holds a lane.
+template <int BLOCK>
+__device__ __forceinline__ void route_lane(BlockShared<BLOCK>& sh, bool active, int lane, int ln) {
+  const int nq = active ? next_queue(sh.lane[lane]) : -3;
+  __threadfence_block();  // the lane's state is written before another warp can take it
+  const unsigned peers = __match_any_sync(0xFFFFFFFFu, nq);
+  if (nq >= 0) {
+    const int leader = __ffs(peers) - 1;
+    const int rank = __popc(peers & ((1u << ln) - 1));
+    unsigned slot = 0;
+    if (ln == leader) slot = atomicAdd(&sh.qtail[nq], (unsigned)__popc(peers));
+    slot = __shfl_sync(peers, slot, leader) + rank;
+    reinterpret_cast<volatile uint16_t*>(sh.q[nq])[slot % BLOCK] = (uint16_t)(lane + 1);
+  } else if (nq == -1) {
+    atomicOr(&sh.parked[lane >> 5], 1u << (lane & 31));
+  } else if (nq == -2) {
+    if (ln == __ffs(peers) - 1) atomicSub(&sh.live, __popc(peers));
+  }
+}
+
+// The queue kernel: the same stages and phases as batch_kernel, without block barriers.
+// Each warp loops on its own: it takes up to 32 lanes from the fullest phase queue of its
+// block, runs that phase for them and hands each lane to the queue of its next stage.
+// Warps never wait for each other (no __syncthreads in the loop), a lane's next stage can
+// run as soon as any warp is free, and a phase with few lanes costs only those lanes.
+template <int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) queue_kernel(BatchArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  BlockShared<BLOCK>& sh = *reinterpret_cast<BlockShared<BLOCK>*>(smem_raw);
+  const int tid = threadIdx.x, ln = tid & 31;
+  const long long base = (long long)blockIdx.x * BLOCK;
+  memset(&sh.cnt[tid], 0, sizeof(LaneCounters));
+  {
+    Lane& L = sh.lane[tid];
+    L.stage = ST_TAKE;
+    L.sp = 0;
+    L.gen = a.lane_gen[base + tid];
+    L.v = 0;
+    L.r = 0;
+    L.p.trick = 0;
+    L.task = -1;
+    sh.q[PH_CHEAP][tid] = (uint16_t)(tid + 1);
+    for (int p = 1; p < PH_COUNT; p++) sh.q[p][tid] = 0;
+  }
+  if (tid < PH_COUNT) {
+    sh.ph_warps[tid] = 0;
+    sh.ph_items[tid] = 0;
+    sh.ph_cycles[tid] = 0;
+    sh.qhead[tid] = 0;
+    sh.qtail[tid] = tid == PH_CHEAP ? BLOCK : 0;
+  }
+  if (tid < BLOCK / 32) sh.parked[tid] = 0;
+  if (tid == 0) {
+    sh.args = a;
+    sh.stop = 0;
+    sh.iters = 0;
+    sh.help_hint = 0;
+    sh.claim_slots = 0;
+    sh.all_done = 0;
+    sh.free_rounds = 0;
+    sh.free_cycles = 0;
+    sh.live = BLOCK;
+    sh.fault = 0;
+  }
+  __syncthreads();
+  volatile unsigned* vhead = sh.qhead;
+  volatile unsigned* vtail = sh.qtail;
+  volatile int* vlive = &sh.live;
+  volatile int* vstop = &sh.stop;
+  volatile int* vfault = &sh.fault;
+  unsigned poll_word = (unsigned)(tid >> 5);
+  for (unsigned loop = 0;; loop++) {
+    if (__shfl_sync(0xFFFFFFFFu, (*vstop | *vfault), 0)) break;  // warp-uniform
+    if (ln == 0 && (loop & 63u) == 63u && a.stop && *a.stop) sh.stop = 1;
+    if (a.tasks && ln == 0 && (loop & 15u) == 0) {
+      const int q = atom_load(&a.tasks->queued), h = atom_load(&a.tasks->hungry);
+      sh.help_hint = h > q;
+      sh.all_done = atom_load(&a.tasks->exhausted) && atom_load(&a.tasks->busy) == 0;
+    }
+    // Lane 0 picks the fullest queue and claims up to 32 of its lanes.
+    int ph = -1;
+    unsigned h0 = 0, n = 0;
+    if (ln == 0) {
+      unsigned best = 0;
+      for (int p = 0; p < PH_COUNT; p++) {
+        const unsigned hd = vhead[p];  // head first: it never passes the tail read after it
+        const unsigned b = vtail[p] - hd;
+        if (b > best) {
+          best = b;
+          ph = p;
+        }
+      }
+      if (ph >= 0) {
+        h0 = vhead[ph];
+        const unsigned avail = vtail[ph] - h0;
+        n = avail < 32u ? avail : 32u;
+        if (n == 0 || atomicCAS(&sh.qhead[ph], h0, h0 + n) != h0) ph = -2;  // lost the race: retry
+      }
+    }
+    ph = __shfl_sync(0xFFFFFFFFu, ph, 0);
+    if (ph == -2) continue;
+    const bool poll = ph < 0 || (loop & 7u) == 7u;
+    if (ph >= 0) {
+      h0 = __shfl_sync(0xFFFFFFFFu, h0, 0);
+      n = __shfl_sync(0xFFFFFFFFu, n, 0);
+      int lane = -1;
+      if ((unsigned)ln < n) {
+        volatile uint16_t* slot = reinterpret_cast<volatile uint16_t*>(sh.q[ph]) + ((h0 + ln) % BLOCK);
+        unsigned v = 0;
+        for (int k = 0; k < (1 << 20) && (v = *slot) == 0; k++) {
+        }
+        if (v == 0) {
+          *vfault = 1;  // the producer never wrote the slot: give up on the whole block
+        } else {
+          *slot = 0;
+          lane = (int)v - 1;
+        }
+        __threadfence_block();  // read the lane's state only after taking it
+      }
+      const long long t0 = clock64();
+      if (lane >= 0) {
+        DevEnv env = lane_env(sh, base + lane, lane);
+        Lane& L = sh.lane[lane];
+        if (ph == PH_CHEAP) {
+          if (env.tp && task_abandoned(L, env.tp)) abort_task(L, env);
+          advance_cheap(L, env);
+        } else if (ph == PH_LEAD || ph == PH_FOLLOW) {
+          step_enter(L, env);
+        } else {
+          step_moves(L, env);
+          step_next(L, env);
+        }
+      }
+      route_lane(sh, lane >= 0, lane, ln);
+      if (ln == 0) {
+        atomicAdd(&sh.ph_items[ph], (unsigned long long)n);
+        atomicAdd(&sh.ph_warps[ph], 1ull);
+        atomicAdd(&sh.ph_cycles[ph], (unsigned long long)(clock64() - t0));
+        atomicAdd(&sh.iters, 1ull);
+      }
+    }
+    if (poll) {
+      // Lanes parked on the task pool: one word of the block at a time.
+      poll_word = (poll_word + 1) % (BLOCK / 32);
+      unsigned m = 0;
+      if (ln == 0 && reinterpret_cast<volatile unsigned*>(sh.parked)[poll_word])
+        m = atomicExch(&sh.parked[poll_word], 0u);
+      m = __shfl_sync(0xFFFFFFFFu, m, 0);
+      __threadfence_block();
+      int lane = -1;
+      if (m) {
+        const int c = __popc(m);
+        if (ln < c) lane = (int)(poll_word * 32 + select_bit(m, ln));
+        // Hungry lanes look for a task only as far as tasks are queued.
+        const unsigned hm = __ballot_sync(0xFFFFFFFFu, lane >= 0 && sh.lane[lane].stage == ST_HUNGRY);
+        int quota = 0;
+        if (ln == 0 && hm) quota = atom_load(&a.tasks->queued);
+        quota = __shfl_sync(0xFFFFFFFFu, quota, 0);
+        if (lane >= 0) {
+          DevEnv env = lane_env(sh, base + lane, lane);
+          Lane& L = sh.lane[lane];
+          if (env.tp && task_abandoned(L, env.tp)) abort_task(L, env);
+          if (L.stage == ST_HUNGRY) {
+            if (*reinterpret_cast<volatile int*>(&sh.all_done)) {
+              atomicAdd(&env.tp->hungry, -1);
+              L.stage = ST_IDLE;
+            } else if (__popc(hm & ((1u << ln) - 1)) < quota) {
+              advance_cheap(L, env);
+            }
+          } else {
+            advance_cheap(L, env);
+          }
+        }
+        route_lane(sh, lane >= 0, lane, ln);
+      } else if (ph < 0) {
+        if (__shfl_sync(0xFFFFFFFFu, *vlive, 0) == 0) break;
+        __nanosleep(256);
+      }
+    }
+  }
+  __syncthreads();
+  a.lane_gen[base + tid] = sh.lane[tid].gen;
+  if (tid == 0 && sh.fault) atomicAdd(a.counters + CNT_FAULTS, 1ull);
+  __syncthreads();
+  block_counters(sh, a, tid);
+}
+
+template <int BLOCK>
+__device__ __forceinline__ void block_counters(BlockShared<BLOCK>& sh, const BatchArgs& a, int tid) {
   // Block sums of the counters, one atomic per word per block.
   if (tid < CNT_WORDS) {
     unsigned long long sum = 0;

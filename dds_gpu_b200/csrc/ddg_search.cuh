@@ -376,6 +376,7 @@ struct Task {
   int8_t target;    // the null-window target of the donor's search
   int8_t v;         // result: value of the donated part
   int8_t best;      // result: the cutting card, or -1
+  u64 key;          // (deal << 3 | strain) + 1 of the donor: helpers keep their TT per key
 };
 
 // The tasks of a launch and the counters that steer helping (HBM on the GPU).
@@ -682,6 +683,7 @@ DDG_CALL void step_take(Lane& L, Env& env) {
   L.p.trump = strain_trump(L.strain);
   L.p.trick = 0;
   L.gen = tt_next_gen(env.tt, env.mask, L.gen);
+  env.tt_key() = 0;
   L.stage = ST_ROOT;
 }
 
@@ -867,7 +869,15 @@ DDG_CALL bool step_hungry(Lane& L, Env& env) {
   L.par_sp = -1;
   L.target = k.target;
   L.task = (int16_t)t;
-  L.gen = tt_next_gen(env.tt, env.mask, L.gen);
+  L.deal = (long long)((k.key - 1) >> 3);
+  L.strain = (int8_t)((k.key - 1) & 7);
+  // Entries of the TT are facts about positions of one deal and trump suit: a helper that
+  // stays on the same (deal, strain) keeps them, which spares it re-searching the subtrees
+  // its earlier tasks already solved.
+  if (env.tt_key() != k.key) {
+    L.gen = tt_next_gen(env.tt, env.mask, L.gen);
+    env.tt_key() = k.key;
+  }
   L.stage = ST_NEXT;
   return true;
 }
@@ -928,6 +938,7 @@ DDG_CALL bool try_donate(Lane& L, Env& env) {
     t.tried = g.tried & ~card_bit(fr_move(g, i));
     t.info = g.info;
     t.target = L.target;
+    t.key = ((u64)L.deal << 3 | (u64)L.strain) + 1;
     t.r = 0;
     t.v = 0;
     t.best = -1;

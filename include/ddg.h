@@ -42,9 +42,12 @@ typedef struct ddg_config {
   int block;            /* threads per block, multiple of 32; default 128 */
   int jobs_per_deal;    /* 5 = one job per strain, the 4 leads share a TT; 20 = one per lead */
   int device;           /* CUDA device ordinal */
-  int schedule;         /* stage order of the warp loop: 0 = RET, NEXT, ROOT, TAKE, then ENTER */
+  int schedule;         /* 0: block-phase kernel (all warps of a block run each stage phase
+                           in turn over the block's compacted lanes); 1: queue kernel (each
+                           warp takes up to 32 lanes from the fullest per-stage queue of its
+                           block, no block barriers) */
   int min_blocks;       /* resident blocks per SM the kernel is compiled for (register cap):
-                           block 128: 1, 4, 6, 8; block 256: 1..4; 0 = 1 */
+                           block 64: 1; block 128: 1, 4, 6; block 256: 1..3; 0 = 1 */
   double time_limit_s;  /* stop after this many seconds (unfinished results = 255); 0 = none */
   double mem_fraction;  /* largest share of free device memory the pool may take; default 0.85 */
   int help;             /* 1: once the job queue is empty, idle lanes take over untried sibling

@@ -35,6 +35,8 @@ struct HostEnv {
   int claim_start() { return 0; }
   u64 work_nodes() { return st.nodes - start_nodes; }
   void task_started() { start_nodes = st.nodes; }
+  u64 tt_key_ = 0;
+  u64& tt_key() { return tt_key_; }
 
   bool take(Lane& L) {
     long long job = (*next)++;
