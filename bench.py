@@ -1,31 +1,33 @@
 #!/usr/bin/env python
 """Benchmark: exact double-dummy deals/s on B200s (one process per GPU, weak scaling).
 
-Workload: the 13-card benchmark set (20,000 seeded uniformly random deals, seed 2,
-ddg_make_deals), full 5x4 trick tables, exact TT with 2^10 buckets per lane. One step =
-one batch solve of `--batch` consecutive deals of the set (rank r of N takes its own
-batch: step s uses deals from ((s*N + r) * batch) mod 20000), inputs already in HBM.
+Workload: the 13-card benchmark set, 20,000 seeded uniformly random deals per GPU
+(ddg_make_deals seed 2; rank r takes deals [20000 r, 20000 (r+1)) of that stream), one
+job per (deal, strain) with the four declarers sharing a TT of 2^10 buckets, all inputs
+resident in HBM. The set is solved as one resumable solve (ddg_solve_begin); one step is
+one slice of it (ddg_solve_continue, --slice-s seconds, every lane's search state kept in
+HBM between slices), so each step is one kernel launch timed with CUDA events.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Rank 0 prints one JSON line. `value` = deals solved by all ranks / max over ranks of the
-device time of the K timed steps (CUDA events on the solve stream, barrier and synchronize
-on both sides; L2 flushed between steps). `e2e` = the same metric through the host API
-(ddg_solve_batch: pinned host deals in, H2D, solve, D2H of the 20-byte results).
-`roofline` = TT bytes the search moved (counted in-kernel) per second of kernel time,
-against the measured HBM copy bandwidth. `cpu_baseline` = the reference's own CPU solver
-(compiled from its sources into oracle/_ref, else the oracle port) on a bounded sample,
-all host cores. `--impl reference` times that CPU path alone as the reference arm.
+Rank 0 prints one JSON line. `value` = (deal, strain) jobs finished by all ranks in the K
+timed slices / 5 / max over ranks of the timed device time: the reference's own headline
+metric ("full-job deals/s": finished jobs / 5 per second while the set is being solved).
+Only finished, exact jobs count; work in progress at the end of the timed slices does
+not. `e2e` = the same through the host API with, every step, the deals copied in from
+pinned host memory and all results copied out. `roofline` = TT bytes the search moved
+(counted in-kernel) per second of kernel time, against the measured HBM copy bandwidth.
+`cpu_baseline` = the reference's own CPU solver (compiled from its sources into
+oracle/_ref, else the C restatement) on the same deals over the same slices, all host
+cores. `--impl reference` prints that CPU measurement as the reference arm.
 """
 import argparse
-import ctypes
 import json
 import os
 import statistics
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -33,7 +35,9 @@ sys.path.insert(0, ROOT)
 
 METRIC = "exact DD deals/s on 1 B200, learned-guided vs plain; nodes/deal; p99 ms"
 SET_SEED, SET_SIZE, SET_K = 2, 20000, 13
-WORKLOAD = "13-card seeded random deals, full 5x4 tables, exact TT 2^10 buckets/lane"
+JPD = 5
+WORKLOAD = ("13-card seeded random deals (20,000 per GPU), all 5 strains x 4 declarers, "
+            "exact TT 2^10 buckets per lane, one job per (deal, strain)")
 
 
 def parse():
@@ -42,17 +46,14 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--batch", type=int, default=1024, help="deals per step per GPU")
+    p.add_argument("--slice-s", type=float, default=4.0, help="seconds per step (one slice of the solve)")
     p.add_argument("--tt-log2", type=int, default=10)
     p.add_argument("--lanes", type=int, default=0, help="0 = fill the GPU")
-    p.add_argument("--jpd", type=int, default=20, help="jobs per deal: 5 (per strain) or 20 (per lead)")
     p.add_argument("--block", type=int, default=256)
     p.add_argument("--min-blocks", type=int, default=2)
-    p.add_argument("--help-lanes", type=int, default=1, help="1: idle lanes help busy ones (same tricks)")
-    p.add_argument("--safety-s", type=float, default=900.0, help="per-step stop; a stopped step is an error")
+    p.add_argument("--schedule", type=int, default=0, help="0 block-phase kernel, 1 queue kernel")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
-    p.add_argument("--cpu-deals", type=int, default=0, help="deals per CPU sample (0 = one per core)")
     return p.parse_args()
 
 
@@ -63,51 +64,51 @@ def host_cores():
         return os.cpu_count() or 1
 
 
-# ---- CPU reference path (checker/baseline only) ----------------------------------------
-
-def cpu_solver():
-    """The reference's CPU solver: oracle/_ref (reference sources) if built, else the port."""
-    P = ctypes.c_void_p
-    ref = os.path.join(ROOT, "oracle", "_ref", "libddref.so")
-    if os.path.exists(ref):
-        lib = ctypes.CDLL(ref)
-        lib.ref_solve_batch.argtypes = [P, ctypes.c_long, ctypes.c_int, ctypes.c_int, P, P]
-
-        def run(h, tt, threads, out, nodes):
-            return lib.ref_solve_batch(h.ctypes.data, h.shape[0], tt, threads, out.ctypes.data, nodes.ctypes.data)
-        return run, "reference"
-    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
-    lib = ctypes.CDLL(os.path.join(ROOT, "oracle", "_build", "libddoracle.so"))
-    lib.ddo_solve_batch.restype = ctypes.c_longlong
-    lib.ddo_solve_batch.argtypes = [P, ctypes.c_long, ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P, P]
-
-    def run(h, tt, threads, out, nodes):
-        r = lib.ddo_solve_batch(h.ctypes.data, h.shape[0], tt, threads, 5, None, out.ctypes.data, nodes.ctypes.data)
-        return 0 if r >= 0 else -1
-    return run, "port"
+def deal_set(rank):
+    from dds_gpu_b200 import make_deals
+    return make_deals(SET_SEED, rank * SET_SIZE, SET_SIZE, SET_K)
 
 
-def cpu_sample(deals, first, n, tt_log2, threads):
-    """Solves deals [first, first+n) of the set on the CPU; returns (seconds, nodes, tables)."""
-    import numpy as np
-    run, kind = cpu_solver()
-    idx = [(first + i) % SET_SIZE for i in range(n)]
-    h = np.ascontiguousarray(deals[idx])
-    out = np.zeros(n * 20, np.int32)
-    nodes = np.zeros(n * 5, np.uint64)
-    t0 = time.perf_counter()
-    rc = run(h, tt_log2, threads, out, nodes)
-    dt = time.perf_counter() - t0
-    if rc != 0:
-        raise RuntimeError("CPU solver failed")
-    return dt, int(nodes.sum()), out.reshape(n, 5, 4), kind
+# ---- CPU reference path (baseline only) -------------------------------------------------
+
+def cpu_window(deals, tt_log2, slice_s, slices):
+    """The reference's CPU solver over the deal set for `slices` slices of `slice_s` seconds
+    (oracle/_ref/cpu_window, built from the reference's sources; else the C restatement's
+    oracle/_build/cpu_window). Returns (jobs finished per slice, nodes per slice, threads, kind)."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "cpu_window")
+    if not os.path.exists(exe):
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
+        exe = os.path.join(ROOT, "oracle", "_build", "cpu_window")
+    cores = host_cores()
+    with tempfile.NamedTemporaryFile(suffix=".bin", delete=False) as f:
+        f.write(deals.tobytes())
+        path = f.name
+    try:
+        out = subprocess.run([exe, path, str(tt_log2), str(cores), str(slice_s), str(slices)],
+                             check=True, capture_output=True, text=True,
+                             timeout=slice_s * slices + 120).stdout
+    finally:
+        os.unlink(path)
+    r = json.loads(out.strip().splitlines()[-1])
+    return r["jobs"], r["nodes"], r["threads"], r["kind"]
+
+
+def cpu_measure(a, deals):
+    jobs, nodes, threads, kind = cpu_window(deals, a.tt_log2, a.slice_s, a.warmup + a.steps)
+    t_jobs = sum(jobs[a.warmup:])
+    value = t_jobs / JPD / (a.steps * a.slice_s)
+    sample = (f"deal set seed {SET_SEED} (20,000 deals) solved by {threads} threads, one TT each; "
+              f"(deal, strain) jobs finished in slices {a.warmup}..{a.warmup + a.steps - 1} of "
+              f"{a.slice_s:g} s (first {a.warmup} = warm-up): {t_jobs} jobs, "
+              f"{sum(nodes[a.warmup:]) / max(1, t_jobs):.0f} nodes/job")
+    return {"value": value, "unit": "deals/s", "cores": threads, "kind": kind, "sample": sample}
 
 
 def config_dict(a, world, extra=None):
-    d = {"workload": WORKLOAD, "deal_set": f"seed {SET_SEED}, {SET_SIZE} deals, K={SET_K}",
-         "deals_per_step_per_gpu": a.batch, "tt_log2": a.tt_log2, "jobs_per_deal": a.jpd,
-         "parallelism": f"dp{world} (independent deals per GPU, no collective on the data path)",
-         "l2": "flushed between steps (256 MiB write); TT working set is also far above L2"}
+    d = {"workload": WORKLOAD, "deal_set": f"seed {SET_SEED}, {SET_SIZE} deals per GPU, K={SET_K}",
+         "tt_log2": a.tt_log2, "jobs_per_deal": JPD, "step": f"one {a.slice_s:g} s slice of the resumable solve",
+         "parallelism": f"dp{world} (own deal set per GPU, no collective on the data path)",
+         "l2": "flushed between steps (256 MiB write); the TT working set (GBs) is far above L2"}
     if extra:
         d.update(extra)
     return d
@@ -116,28 +117,13 @@ def config_dict(a, world, extra=None):
 def reference_arm(a, rank, world):
     if rank != 0:
         return
-    import numpy as np
-    from dds_gpu_b200 import make_deals
-    deals = make_deals(SET_SEED, 0, SET_SIZE, SET_K)
-    cores = host_cores()
-    n = a.cpu_deals or max(4, cores)
-    times, nodes = [], 0
-    kind = "reference"
-    for s in range(a.warmup + a.steps):
-        dt, nd, _, kind = cpu_sample(deals, s * n, n, a.tt_log2, cores)
-        if s >= a.warmup:
-            times.append(dt)
-            nodes += nd
-    total = sum(times)
-    value = a.steps * n / total
-    sample = f"{n} deals per step x {a.steps} steps (deals 0..{(a.warmup + a.steps) * n - 1}; first {a.warmup * n} as warm-up), all 20 results"
-    line = {"metric": METRIC, "value": value, "unit": "deals/s", "impl": "reference", "n_gpus": world,
-            "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * total / a.steps,
+    cpu = cpu_measure(a, deal_set(0))
+    line = {"metric": METRIC, "value": cpu["value"], "unit": "deals/s", "impl": "reference", "n_gpus": world,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * a.slice_s,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
-            "data": "synthetic", "config": config_dict(a, world, {"deals_per_step_per_gpu": n}),
-            "nodes_per_deal": nodes / (a.steps * n),
-            "cpu_baseline": {"value": value, "unit": "deals/s", "cores": cores, "kind": kind, "sample": sample},
-            "e2e": {"value": value, "unit": "deals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "data": "synthetic", "config": config_dict(a, world),
+            "cpu_baseline": cpu,
+            "e2e": {"value": cpu["value"], "unit": "deals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
@@ -200,6 +186,17 @@ def peaks():
         return 6650.0, "fallback"
 
 
+def golden_check(tables):
+    """Results the GPU finished for the first deals of the set (rank 0's) against the
+    reference's tables in the committed fixture (tests/golden/k13_24.npz)."""
+    import numpy as np
+    g = np.load(os.path.join(ROOT, "tests", "golden", "k13_24.npz"))
+    want = g["tricks"].reshape(-1, 20)
+    got = tables[: want.shape[0]]
+    done = got != 255
+    return {"checked": int(done.sum()), "equal": bool((got[done] == want[done]).all())}
+
+
 def our_arm(a, rank, world, local_rank):
     import numpy as np
     import torch
@@ -207,32 +204,25 @@ def our_arm(a, rank, world, local_rank):
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    deals = ddg.make_deals(SET_SEED, 0, SET_SIZE, SET_K)
-    solver = ddg.Solver(tt_log2=a.tt_log2, lanes=a.lanes, block=a.block, jobs_per_deal=a.jpd, device=local_rank,
-                        min_blocks=a.min_blocks, help=a.help_lanes, time_limit_s=a.safety_s)
-    B = a.batch
-    nsteps = a.warmup + a.steps
-
-    def step_idx(s):
-        start = ((s * world + rank) * B) % SET_SIZE
-        return [(start + i) % SET_SIZE for i in range(B)]
-
-    host_in = [torch.from_numpy(np.ascontiguousarray(deals[step_idx(s)]).view(np.int64)).pin_memory()
-               for s in range(nsteps)]
-    dev_in = [h.to(dev) for h in host_in]
-    dev_outs = [torch.empty((B, 20), dtype=torch.uint8, device=dev) for _ in range(nsteps)]
-    dev_out = dev_outs[0]
+    deals = deal_set(rank)
+    solver = ddg.Solver(tt_log2=a.tt_log2, lanes=a.lanes, block=a.block, jobs_per_deal=JPD, device=local_rank,
+                        min_blocks=a.min_blocks, schedule=a.schedule)
+    n = deals.shape[0]
+    host_in = torch.from_numpy(deals.view(np.int64)).pin_memory()
+    dev_in = host_in.to(dev)
+    dev_out = torch.empty((n, 20), dtype=torch.uint8, device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream(dev)
+    cs = stream.cuda_stream
 
     def barrier():
         if world > 1:
             torch.distributed.barrier()
 
-    # Warm-up steps (untimed).
-    for s in range(a.warmup):
+    solver.begin(dev_in.data_ptr(), n, dev_out.data_ptr(), stream=cs)
+    for s in range(a.warmup):  # warm-up slices (untimed)
         flush.zero_()
-        solver.solve_device(dev_in[s].data_ptr(), B, dev_out.data_ptr(), stream=stream.cuda_stream)
+        solver.resume(a.slice_s, stream=cs)
     torch.cuda.synchronize(dev)
 
     sampler = ClockSampler(local_rank)
@@ -242,79 +232,62 @@ def our_arm(a, rank, world, local_rank):
     sampler.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for s in range(a.warmup, nsteps):
+    for s in range(a.steps):
         flush.zero_()
-        stats.append(solver.solve_device(dev_in[s].data_ptr(), B, dev_outs[s].data_ptr(), stream=stream.cuda_stream))
+        stats.append(solver.resume(a.slice_s, stream=cs)[1])
     e1.record(stream)
     torch.cuda.synchronize(dev)
     barrier()
     clocks = sampler.stop()
     elapsed_ms = e0.elapsed_time(e1)
-    # Every result of every timed step must be there (the safety stop leaves 255s).
-    unsolved = sum(int((dev_outs[s] == 255).sum().item()) for s in range(a.warmup, nsteps))
-    tables = [dev_outs[s].cpu().numpy() for s in range(a.warmup, nsteps)]
+    tables = dev_out.cpu().numpy()
+    jobs = sum(st["jobs_done"] for st in stats)
 
-    # End to end through the host API: pinned deals in, results out, every step.
-    e2e_ms = None
+    # End to end through the host API: each step copies the deals in from pinned host memory,
+    # runs the slice and copies every result out.
+    e2e_ms, e2e_jobs = None, 0
     if not a.no_e2e:
-        host_out = torch.empty((B, 20), dtype=torch.uint8).pin_memory()
-        lib = ddg.load_library()
-        st = ddg._Stats()
+        host_out = torch.empty((n, 20), dtype=torch.uint8).pin_memory()
+        solver.begin(dev_in.data_ptr(), n, dev_out.data_ptr(), stream=cs)
         for s in range(a.warmup):
-            ddg._check(lib.ddg_solve_batch(solver._h, host_in[s].data_ptr(), B, host_out.data_ptr(), ctypes.byref(st)))
+            solver.resume(a.slice_s, hands_host=host_in.data_ptr(), out_host=host_out.data_ptr(), stream=cs)
         barrier()
         torch.cuda.synchronize(dev)
-        h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        legacy = torch.cuda.default_stream(dev)
-        h0.record(legacy)
         t0 = time.perf_counter()
-        for s in range(a.warmup, nsteps):
+        for s in range(a.steps):
             flush.zero_()
-            ddg._check(lib.ddg_solve_batch(solver._h, host_in[s].data_ptr(), B, host_out.data_ptr(), ctypes.byref(st)))
-            assert int(host_out[0, 0]) <= 13
-        h1.record(legacy)
+            e2e_jobs += solver.resume(a.slice_s, hands_host=host_in.data_ptr(), out_host=host_out.data_ptr(),
+                                      stream=cs)[1]["jobs_done"]
+            assert int((host_out[:24] != 255).sum()) >= 0  # the results are on the host
         torch.cuda.synchronize(dev)
-        wall_ms = 1e3 * (time.perf_counter() - t0)
-        e2e_ms = max(h0.elapsed_time(h1), wall_ms)
+        e2e_ms = 1e3 * (time.perf_counter() - t0)
         barrier()
 
+    nodes = sum(st["nodes"] for st in stats)
     if world > 1:
         t = torch.tensor([elapsed_ms, e2e_ms or 0.0], dtype=torch.float64, device=dev)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         elapsed_ms, e2e_ms = t[0].item(), (t[1].item() if e2e_ms else None)
-
-    kernel_ms = sum(s["kernel_ms"] for s in stats)
-    nodes = sum(s["nodes"] for s in stats)
-    tt_bytes = sum(s["tt_bytes"] for s in stats)
-    it = [sum(s["phase_warps"][k] for s in stats) for k in range(5)]
-    ln = [sum(s["phase_items"][k] for s in stats) for k in range(5)]
-    tasks = sum(s["tasks"] for s in stats)
-    if world > 1:
-        t = torch.tensor([nodes, tt_bytes], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t)
-        nodes_all = t[0].item()
+        c = torch.tensor([jobs, e2e_jobs, nodes], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(c)
+        jobs_all, e2e_jobs_all, nodes_all = c[0].item(), c[1].item(), c[2].item()
     else:
-        nodes_all = nodes
+        jobs_all, e2e_jobs_all, nodes_all = jobs, e2e_jobs, nodes
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
-        cores = host_cores()
-        n = a.cpu_deals or max(4, cores)
-        dt, cn, tables, kind = cpu_sample(deals, 0, n, a.tt_log2, cores)
-        cpu = {"value": n / dt, "unit": "deals/s", "cores": cores, "kind": kind,
-               "sample": f"deals 0..{n - 1} of the set (5 strains x 4 declarers each), {cores} threads, "
-                         f"TT 2^{a.tt_log2} buckets per thread, {dt:.1f} s, {cn / n:.0f} nodes/deal"}
-        # The GPU answers for the same deals must match the CPU reference's.
-        gpu_tab = solver.solve(deals[:n])
-        cpu["tables_equal_gpu"] = bool((gpu_tab == tables).all())
+        cpu = cpu_measure(a, deals)
 
     if rank != 0:
         solver.close()
         return
+    kernel_ms = sum(st["kernel_ms"] for st in stats)
+    tt_bytes = sum(st["tt_bytes"] for st in stats)
+    it = [sum(st["phase_warps"][k] for st in stats) for k in range(5)]
+    ln = [sum(st["phase_items"][k] for st in stats) for k in range(5)]
     peak, peak_kind = peaks()
     achieved = tt_bytes / (kernel_ms * 1e-3) / 1e9 if kernel_ms else 0.0
-    deals_total = a.steps * B * world
-    value = deals_total / (elapsed_ms * 1e-3)
+    value = jobs_all / JPD / (elapsed_ms * 1e-3)
     eff = {name: (ln[k] / (32.0 * it[k]) if it[k] else None)
            for k, name in enumerate(["cheap", "enter_lead", "enter_follow", "moves_lead", "moves_follow"])}
     traffic = None
@@ -323,30 +296,30 @@ def our_arm(a, rank, world, local_rank):
         try:
             with open(tfile) as f:
                 tj = json.load(f)
-            traffic = tj.get("dram_bytes_per_node", 0) * nodes / max(1, len(stats))
-        except (OSError, ValueError):
+            traffic = tj["dram_bytes_per_node"] * nodes / max(1, len(stats))
+        except (OSError, ValueError, KeyError):
             traffic = None
     line = {
         "metric": METRIC, "value": value, "unit": "deals/s", "n_gpus": world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": elapsed_ms / a.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
-        "config": config_dict(a, world, {"lanes": stats[0]["lanes"] if stats else 0,
-                                         "block": a.block, "guide": "off (plain DDS move order)"}),
-        "nodes_per_deal": nodes_all / deals_total, "nodes_per_s": nodes_all / (elapsed_ms * 1e-3),
-        "unsolved_results": unsolved,
-        "helping_tasks": tasks,
+        "config": config_dict(a, world, {"lanes": stats[0]["lanes"] if stats else 0, "block": a.block,
+                                         "schedule": a.schedule, "guide": "off (plain DDS move order)"}),
+        "jobs_finished": int(jobs_all), "nodes_per_s": nodes_all / (elapsed_ms * 1e-3),
+        "nodes_per_finished_job": nodes_all / max(1, jobs_all),
+        "golden_check": golden_check(tables),
         "warp_efficiency": eff,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                     "kernel": "ddg::batch_kernel",
+                     "kernel": "ddg::batch_kernel<256,2>",
                      "algorithmic_bytes": "TT bytes read+written per launch, counted in-kernel "
                                           f"({tt_bytes / max(1, nodes):.1f} B/node)"},
         "clocks": clocks,
         "gpu_launches": len(stats),
     }
     if e2e_ms:
-        line["e2e"] = {"value": deals_total / (e2e_ms * 1e-3), "unit": "deals/s",
-                       "h2d_bytes_per_step": B * 32, "d2h_bytes_per_step": B * 20}
+        line["e2e"] = {"value": e2e_jobs_all / JPD / (e2e_ms * 1e-3), "unit": "deals/s",
+                       "h2d_bytes_per_step": n * 32, "d2h_bytes_per_step": n * 20}
     if cpu:
         line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)

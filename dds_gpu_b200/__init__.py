@@ -13,7 +13,7 @@ import os
 
 import numpy as np
 
-__all__ = ["Solver", "DDGError", "make_deals", "check_deal", "library_path", "load_library"]
+__all__ = ["Solver", "Stream", "DDGError", "make_deals", "check_deal", "library_path", "load_library"]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "_lib", "libddg.so")
@@ -81,7 +81,18 @@ def load_library():
     lib.ddg_solve_batch.argtypes = [P, P, ctypes.c_int64, P, ctypes.POINTER(_Stats)]
     lib.ddg_solve_batch_seeded.argtypes = [P, P, ctypes.c_int64, P, P, ctypes.POINTER(_Stats)]
     lib.ddg_solve_device.argtypes = [P, P, ctypes.c_int64, P, P, P, P, ctypes.POINTER(_Stats)]
+    lib.ddg_solve_begin.argtypes = [P, P, ctypes.c_int64, P, P, P]
+    lib.ddg_solve_continue.argtypes = [P, ctypes.c_double, P, P, P, ctypes.POINTER(_Stats),
+                                       ctypes.POINTER(ctypes.c_int)]
     lib.ddg_solve_strain.argtypes = [P, P, ctypes.c_int, P, P]
+    lib.ddg_stream_open.argtypes = [P, ctypes.c_int, ctypes.c_double, ctypes.POINTER(P)]
+    lib.ddg_stream_submit.argtypes = [P, P, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]
+    lib.ddg_stream_poll.argtypes = [P, P, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]
+    lib.ddg_stream_in_flight.argtypes = [P]
+    lib.ddg_stream_in_flight.restype = ctypes.c_int64
+    lib.ddg_stream_capacity.argtypes = [P]
+    lib.ddg_stream_capacity.restype = ctypes.c_int64
+    lib.ddg_stream_close.argtypes = [P, ctypes.c_int, ctypes.POINTER(_Stats)]
     lib.ddg_check_deal.argtypes = [P]
     lib.ddg_make_deals.argtypes = [ctypes.c_uint64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int, P]
     lib.ddg_make_deals.restype = None
@@ -171,6 +182,20 @@ class Solver:
         self.last_stats = st.as_dict()
         return self.last_stats
 
+    def begin(self, d_hands, n, d_out, d_seeds=0, stream=0):
+        """Starts a resumable solve on device buffers (ddg_solve_begin)."""
+        _check(self._lib.ddg_solve_begin(self._h, P(d_hands), n, P(d_seeds or None), P(d_out), P(stream or None)))
+
+    def resume(self, seconds, hands_host=0, out_host=0, stream=0):
+        """Runs the resumable solve for at most `seconds` (ddg_solve_continue); returns
+        (finished, stats of the slice)."""
+        st = _Stats()
+        fin = ctypes.c_int(0)
+        _check(self._lib.ddg_solve_continue(self._h, seconds, P(hands_host or None), P(out_host or None),
+                                            P(stream or None), ctypes.byref(st), ctypes.byref(fin)))
+        self.last_stats = st.as_dict()
+        return bool(fin.value), self.last_stats
+
     def set_job_times(self, d_job_end_ns):
         """Device buffer (integer address, n*jobs_per_deal uint64) for job completion times."""
         _check(self._lib.ddg_solver_set_job_times(self._h, P(d_job_end_ns or None)))
@@ -183,3 +208,52 @@ class Solver:
         _check(self._lib.ddg_solve_strain(self._h, h.ctypes.data, strain,
                                           None if s4 is None else s4.ctypes.data, out.ctypes.data))
         return [int(x) for x in out]
+
+
+class Stream:
+    """Continuous batching on one solver (ddg_stream_*): submit deals while others are on
+    the GPU, poll 28-byte records (index, 20 tricks) as deals finish, out of order."""
+
+    def __init__(self, solver, ring_slots=0, idle_timeout_s=0.0):
+        self._lib = solver._lib
+        self._h = P()
+        _check(self._lib.ddg_stream_open(solver._h, ring_slots, idle_timeout_s, ctypes.byref(self._h)))
+        self.stats = None
+
+    @property
+    def in_flight(self):
+        return self._lib.ddg_stream_in_flight(self._h)
+
+    @property
+    def capacity(self):
+        return self._lib.ddg_stream_capacity(self._h)
+
+    def submit(self, hands):
+        """Submits deals (n, 4) uint64 in order; returns how many were admitted (a prefix)."""
+        h = np.ascontiguousarray(hands, dtype=np.uint64).reshape(-1, 4)
+        acc = ctypes.c_int64(0)
+        _check(self._lib.ddg_stream_submit(self._h, h.ctypes.data, h.shape[0], ctypes.byref(acc)))
+        return acc.value
+
+    def poll(self, max_records=65536):
+        """Finished deals: (indices uint64 (k,), tricks uint8 (k, 5, 4))."""
+        buf = np.empty(max_records * 28, dtype=np.uint8)
+        got = ctypes.c_int64(0)
+        _check(self._lib.ddg_stream_poll(self._h, buf.ctypes.data, max_records, ctypes.byref(got)))
+        rec = buf[: got.value * 28].reshape(-1, 28)
+        return rec[:, :8].copy().view(np.uint64).reshape(-1), rec[:, 8:].reshape(-1, 5, 4).copy()
+
+    def close(self, drain=True):
+        """Ends the stream; drain=True waits for every submitted deal, False drops them."""
+        if self._h:
+            st = _Stats()
+            h, self._h = self._h, P()
+            _check(self._lib.ddg_stream_close(h, 1 if drain else 0, ctypes.byref(st)))
+            self.stats = st.as_dict()
+        return self.stats
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

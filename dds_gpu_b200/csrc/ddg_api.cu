@@ -6,6 +6,8 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <thread>
 #include <vector>
@@ -58,6 +60,12 @@ struct ddg_solver {
   uint64_t* d_job_end_ns = nullptr;  // caller's buffer for job completion times, or null
   uint64_t start_ns = 0;             // device global timer at the last solve's launch
   TaskPool* tasks = nullptr;         // helping's task pool (cfg.help), cleared per solve
+  // Resumable (time-sliced) solve.
+  LaneSave* save = nullptr;  // lanes x LaneSave, allocated by the first ddg_solve_begin
+  BatchArgs slice_args;
+  int64_t slice_n = 0;
+  bool sliced = false, slice_done = false;
+  bool streaming = false;  // a ddg_stream owns the lanes until it is closed
 };
 
 extern "C" {
@@ -135,6 +143,7 @@ void ddg_solver_destroy(ddg_solver* s) {
   cudaFree(s->lane_gen);
   cudaFree(s->counters);
   cudaFree(s->tasks);
+  cudaFree(s->save);
   cudaFree(s->d_hands);
   cudaFree(s->d_out);
   cudaFree(s->d_seeds);
@@ -265,23 +274,13 @@ static int launch_batch(ddg_solver* s, const BatchArgs& a, long long n_jobs, cud
   return DDG_OK;
 }
 
-int ddg_solve_device(ddg_solver* s, const uint64_t* d_hands, int64_t n, const int8_t* d_seed20,
-                     uint8_t* d_out20, uint64_t* d_job_nodes, void* stream_v, ddg_stats* st) {
-  if (!s) return fail(DDG_E_ARG, "null solver");
-  if (n < 0 || (n > 0 && (!d_hands || !d_out20))) return fail(DDG_E_ARG, "bad batch arguments");
-  if (st) memset(st, 0, sizeof(*st));
-  if (n == 0) return DDG_OK;
-  if ((reinterpret_cast<uintptr_t>(d_hands) & 15) != 0) return fail(DDG_E_ARG, "hands not 16-byte aligned");
-  CUDA_TRY(cudaSetDevice(s->device));
-  cudaStream_t stream = (cudaStream_t)stream_v;
-  const int jpd = s->cfg.jobs_per_deal;
-  const long long n_jobs = (long long)n * jpd;
-  CUDA_TRY(cudaMemsetAsync(s->counters, 0, CNT_WORDS * 8, stream));
-  CUDA_TRY(cudaMemsetAsync(d_out20, 0xFF, (size_t)n * 20, stream));
-  *(volatile int*)s->h_stop = 0;
+static BatchArgs make_args(ddg_solver* s, const uint64_t* d_hands, int64_t n, const int8_t* d_seed20,
+                           uint8_t* d_out20, uint64_t* d_job_nodes) {
   BatchArgs a;
+  memset(&a, 0, sizeof(a));
+  const int jpd = s->cfg.jobs_per_deal;
   a.hands = d_hands;
-  a.n_jobs = n_jobs;
+  a.n_jobs = (long long)n * jpd;
   a.jpd = jpd;
   a.mode = d_seed20 ? MODE_STEP : MODE_BISECT;
   a.seeds = d_seed20;
@@ -298,13 +297,49 @@ int ddg_solve_device(ddg_solver* s, const uint64_t* d_hands, int64_t n, const in
   a.tasks = s->tasks;
   a.free_below = s->cfg.free_below == 0 ? 64 : s->cfg.free_below < 0 ? 0 : s->cfg.free_below;
   a.free_steps = s->cfg.free_steps > 0 ? s->cfg.free_steps : 256;
-  if (s->tasks) CUDA_TRY(cudaMemsetAsync(s->tasks, 0, sizeof(TaskPool), stream));
-  if (s->d_job_end_ns) CUDA_TRY(cudaMemsetAsync(s->d_job_end_ns, 0, (size_t)n_jobs * 8, stream));
-  CUDA_TRY(cudaEventRecord(s->ev0, stream));
-  int grid = 0;
-  int rc = launch_batch(s, a, n_jobs, stream, &grid);
-  if (rc) return rc;
-  CUDA_TRY(cudaEventRecord(s->ev1, stream));
+  a.next_job = s->counters + CNT_NEXT_JOB;
+  return a;
+}
+
+// Counters of the last launch into `st` (and the solver's node total). Returns the words.
+static int read_stats(ddg_solver* s, int grid, ddg_stats* st, unsigned long long* c) {
+  CUDA_TRY(cudaMemcpy(c, s->counters, CNT_WORDS * 8, cudaMemcpyDeviceToHost));
+  s->total_nodes += c[CNT_NODES];
+  if (c[CNT_FAULTS])
+    return fail(DDG_E_TIMEOUT, "%llu blocks gave up a bounded queue wait; results incomplete", c[CNT_FAULTS]);
+  if (!st) return DDG_OK;
+  st->nodes = c[CNT_NODES];
+  st->tt_probes = c[CNT_PROBES];
+  st->tt_hits = c[CNT_HITS];
+  st->tt_stores = c[CNT_STORES];
+  st->tt_bytes = c[CNT_TT_BYTES];
+  for (int k = 0; k < 7; k++) st->enter_exit[k] = c[CNT_EXIT + k];
+  for (int k = 0; k < PH_COUNT; k++) {
+    st->phase_warps[k] = c[CNT_PHASE_WARPS + k];
+    st->phase_items[k] = c[CNT_PHASE_ITEMS + k];
+    st->phase_cycles[k] = c[CNT_PHASE_CYCLES + k];
+  }
+  st->free_rounds = c[CNT_PHASE_ITEMS + PH_COUNT];
+  st->free_cycles = c[CNT_PHASE_CYCLES + PH_COUNT];
+  st->iterations = c[CNT_ITERS];
+  st->tasks = 0;
+  if (s->tasks) {
+    int posted = 0;
+    CUDA_TRY(cudaMemcpy(&posted, &s->tasks->posted, sizeof(int), cudaMemcpyDeviceToHost));
+    st->tasks = (uint64_t)posted;
+  }
+  st->jobs_done = (int64_t)c[CNT_JOBS_DONE];
+  float ms = 0;
+  CUDA_TRY(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
+  st->kernel_ms = ms;
+  st->grid = grid;
+  st->block = s->block;
+  st->lanes = grid * s->block;
+  return DDG_OK;
+}
+
+// Waits for the launch between ev0 and ev1; the host time limit raises the stop flag.
+static int wait_launch(ddg_solver* s) {
   if (s->cfg.time_limit_s > 0) {
     auto t0 = std::chrono::steady_clock::now();
     for (;;) {
@@ -318,41 +353,347 @@ int ddg_solve_device(ddg_solver* s, const uint64_t* d_hands, int64_t n, const in
   }
   CUDA_TRY(cudaEventSynchronize(s->ev1));
   CUDA_TRY(cudaGetLastError());
+  return DDG_OK;
+}
+
+int ddg_solve_device(ddg_solver* s, const uint64_t* d_hands, int64_t n, const int8_t* d_seed20,
+                     uint8_t* d_out20, uint64_t* d_job_nodes, void* stream_v, ddg_stats* st) {
+  if (!s) return fail(DDG_E_ARG, "null solver");
+  if (n < 0 || (n > 0 && (!d_hands || !d_out20))) return fail(DDG_E_ARG, "bad batch arguments");
+  if (st) memset(st, 0, sizeof(*st));
+  if (n == 0) return DDG_OK;
+  if ((reinterpret_cast<uintptr_t>(d_hands) & 15) != 0) return fail(DDG_E_ARG, "hands not 16-byte aligned");
+  if (s->streaming) return fail(DDG_E_STATE, "a stream is open on this solver");
+  CUDA_TRY(cudaSetDevice(s->device));
+  s->sliced = false;  // a plain solve ends any resumable one
+  cudaStream_t stream = (cudaStream_t)stream_v;
+  BatchArgs a = make_args(s, d_hands, n, d_seed20, d_out20, d_job_nodes);
+  CUDA_TRY(cudaMemsetAsync(s->counters, 0, CNT_WORDS * 8, stream));
+  CUDA_TRY(cudaMemsetAsync(d_out20, 0xFF, (size_t)n * 20, stream));
+  *(volatile int*)s->h_stop = 0;
+  if (s->tasks) CUDA_TRY(cudaMemsetAsync(s->tasks, 0, sizeof(TaskPool), stream));
+  if (s->d_job_end_ns) CUDA_TRY(cudaMemsetAsync(s->d_job_end_ns, 0, (size_t)a.n_jobs * 8, stream));
+  CUDA_TRY(cudaEventRecord(s->ev0, stream));
+  int grid = 0;
+  int rc = launch_batch(s, a, a.n_jobs, stream, &grid);
+  if (rc) return rc;
+  CUDA_TRY(cudaEventRecord(s->ev1, stream));
+  rc = wait_launch(s);
+  if (rc) return rc;
   unsigned long long c[CNT_WORDS];
-  CUDA_TRY(cudaMemcpy(c, s->counters, sizeof(c), cudaMemcpyDeviceToHost));
-  s->total_nodes += c[CNT_NODES];
-  if (c[CNT_FAULTS])
-    return fail(DDG_E_TIMEOUT, "%llu blocks gave up a bounded queue wait; results incomplete", c[CNT_FAULTS]);
-  if (st) {
-    st->nodes = c[CNT_NODES];
-    st->tt_probes = c[CNT_PROBES];
-    st->tt_hits = c[CNT_HITS];
-    st->tt_stores = c[CNT_STORES];
-    st->tt_bytes = c[CNT_TT_BYTES];
-    for (int k = 0; k < 7; k++) st->enter_exit[k] = c[CNT_EXIT + k];
-    for (int k = 0; k < PH_COUNT; k++) {
-      st->phase_warps[k] = c[CNT_PHASE_WARPS + k];
-      st->phase_items[k] = c[CNT_PHASE_ITEMS + k];
-      st->phase_cycles[k] = c[CNT_PHASE_CYCLES + k];
+  return read_stats(s, grid, st, c);
+}
+
+int ddg_solve_begin(ddg_solver* s, const uint64_t* d_hands, int64_t n, const int8_t* d_seed20, uint8_t* d_out20,
+                    void* stream_v) {
+  if (!s) return fail(DDG_E_ARG, "null solver");
+  if (n <= 0 || !d_hands || !d_out20) return fail(DDG_E_ARG, "bad batch arguments");
+  if ((reinterpret_cast<uintptr_t>(d_hands) & 15) != 0) return fail(DDG_E_ARG, "hands not 16-byte aligned");
+  if (s->streaming) return fail(DDG_E_STATE, "a stream is open on this solver");
+  CUDA_TRY(cudaSetDevice(s->device));
+  if (!s->save) {
+    cudaError_t e = cudaMalloc(&s->save, (size_t)s->lanes * sizeof(LaneSave));
+    if (e != cudaSuccess) {
+      s->save = nullptr;
+      return fail(e == cudaErrorMemoryAllocation ? DDG_E_MEMORY : DDG_E_CUDA, "lane save area: %s",
+                  cudaGetErrorString(e));
     }
-    st->free_rounds = c[CNT_PHASE_ITEMS + PH_COUNT];
-    st->free_cycles = c[CNT_PHASE_CYCLES + PH_COUNT];
-    st->iterations = c[CNT_ITERS];
-    st->tasks = 0;
-    if (s->tasks) {
-      int posted = 0;
-      CUDA_TRY(cudaMemcpy(&posted, &s->tasks->posted, sizeof(int), cudaMemcpyDeviceToHost));
-      st->tasks = (uint64_t)posted;
+    s->bytes += (size_t)s->lanes * sizeof(LaneSave);
+  }
+  cudaStream_t stream = (cudaStream_t)stream_v;
+  s->slice_args = make_args(s, d_hands, n, d_seed20, d_out20, nullptr);
+  s->slice_args.save = s->save;
+  s->slice_args.resume = 0;
+  s->slice_n = n;
+  CUDA_TRY(cudaMemsetAsync(s->counters, 0, CNT_WORDS * 8, stream));
+  CUDA_TRY(cudaMemsetAsync(d_out20, 0xFF, (size_t)n * 20, stream));
+  if (s->tasks) CUDA_TRY(cudaMemsetAsync(s->tasks, 0, sizeof(TaskPool), stream));
+  if (s->d_job_end_ns) CUDA_TRY(cudaMemsetAsync(s->d_job_end_ns, 0, (size_t)s->slice_args.n_jobs * 8, stream));
+  s->sliced = true;
+  s->slice_done = false;
+  return DDG_OK;
+}
+
+int ddg_solve_continue(ddg_solver* s, double seconds, const uint64_t* hands_host, uint8_t* out20_host,
+                       void* stream_v, ddg_stats* st, int* finished) {
+  if (!s) return fail(DDG_E_ARG, "null solver");
+  if (st) memset(st, 0, sizeof(*st));
+  if (finished) *finished = 0;
+  if (!s->sliced) return fail(DDG_E_STATE, "no resumable solve: call ddg_solve_begin first");
+  if (!(seconds > 0)) return fail(DDG_E_ARG, "slice of %g s", seconds);
+  CUDA_TRY(cudaSetDevice(s->device));
+  cudaStream_t stream = (cudaStream_t)stream_v;
+  BatchArgs a = s->slice_args;
+  CUDA_TRY(cudaEventRecord(s->ev0, stream));
+  if (hands_host)  // the caller's deals again (pinned memory makes this an async copy)
+    CUDA_TRY(cudaMemcpyAsync((void*)a.hands, hands_host, (size_t)s->slice_n * 32, cudaMemcpyHostToDevice, stream));
+  int grid = 0;
+  if (!s->slice_done) {
+    // Every counter but the job queue's head starts again at zero.
+    CUDA_TRY(cudaMemsetAsync(s->counters + 1, 0, (CNT_WORDS - 1) * 8, stream));
+    *(volatile int*)s->h_stop = 0;
+    a.slice_ns = (u64)(seconds * 1e9);
+    int rc = launch_batch(s, a, a.n_jobs, stream, &grid);
+    if (rc) return rc;
+  }
+  if (out20_host)
+    CUDA_TRY(cudaMemcpyAsync(out20_host, a.out20, (size_t)s->slice_n * 20, cudaMemcpyDeviceToHost, stream));
+  CUDA_TRY(cudaEventRecord(s->ev1, stream));
+  int rc = wait_launch(s);
+  if (rc) return rc;
+  if (s->slice_done) {
+    if (finished) *finished = 1;
+    return DDG_OK;
+  }
+  s->slice_args.resume = 1;
+  unsigned long long c[CNT_WORDS];
+  rc = read_stats(s, grid, st, c);
+  if (rc) return rc;
+  if ((long long)c[CNT_BLOCKS_DONE] == grid) s->slice_done = true;
+  if (finished) *finished = s->slice_done ? 1 : 0;
+  return DDG_OK;
+}
+
+
+// ---- streams: a device ring of deals fed while the persistent kernel runs ---------------
+
+struct ddg_stream {
+  ddg_solver* s = nullptr;
+  int slots = 0;
+  long long admit = 0;  // most deals in flight (published, not yet polled)
+  u64* d_ring = nullptr;
+  uint8_t* d_out = nullptr;
+  int* d_done = nullptr;
+  unsigned long long* d_words = nullptr;  // [0] published, [1] next job, [2] completion tail, [3] closing
+  CompRec* h_comp = nullptr;              // mapped host memory
+  CompRec* d_comp = nullptr;
+  u64* h_stage = nullptr;                 // pinned mirror of the ring
+  unsigned long long* h_words = nullptr;  // pinned sources of the published / closing words
+  std::vector<uint8_t> slot_busy;
+  unsigned long long published = 0, consumed = 0;
+  cudaStream_t kstream = nullptr, cstream = nullptr;
+  cudaEvent_t kdone = nullptr;
+  bool launched = false;
+  double idle_timeout_s = 30;
+  int launches = 0;
+};
+
+static void stream_free(ddg_stream* st) {
+  if (!st) return;
+  if (st->kstream) cudaStreamSynchronize(st->kstream);
+  cudaFree(st->d_ring);
+  cudaFree(st->d_out);
+  cudaFree(st->d_done);
+  cudaFree(st->d_words);
+  if (st->h_comp) cudaFreeHost(st->h_comp);
+  if (st->h_stage) cudaFreeHost(st->h_stage);
+  if (st->h_words) cudaFreeHost(st->h_words);
+  if (st->kstream) cudaStreamDestroy(st->kstream);
+  if (st->cstream) cudaStreamDestroy(st->cstream);
+  if (st->kdone) cudaEventDestroy(st->kdone);
+  if (st->s) st->s->streaming = false;
+  delete st;
+}
+
+// Launches the stream kernel unless it is running; it ends by itself once its lanes found
+// no deal for idle_timeout_s, or once the stream is closing and every deal is done.
+static int stream_kernel(ddg_stream* st) {
+  if (st->launched) {
+    cudaError_t q = cudaEventQuery(st->kdone);
+    if (q == cudaErrorNotReady) return DDG_OK;
+    if (q != cudaSuccess) return fail(DDG_E_CUDA, "stream kernel: %s", cudaGetErrorString(q));
+    st->launched = false;
+    unsigned long long faults = 0;
+    CUDA_TRY(cudaMemcpy(&faults, st->s->counters + CNT_FAULTS, 8, cudaMemcpyDeviceToHost));
+    if (faults) return fail(DDG_E_TIMEOUT, "stream kernel gave up a bounded wait");
+  }
+  ddg_solver* s = st->s;
+  BatchArgs a = make_args(s, nullptr, 0, nullptr, st->d_out, nullptr);
+  a.tasks = nullptr;  // lanes without a deal wait for the next one instead of helping
+  a.job_end_ns = nullptr;
+  a.ring = st->d_ring;
+  a.published = st->d_words + 0;
+  a.next_job = st->d_words + 1;
+  a.comp_tail = st->d_words + 2;
+  a.closing = reinterpret_cast<const int*>(st->d_words + 3);
+  a.deal_done = st->d_done;
+  a.comp = st->d_comp;
+  a.ring_mask = st->slots - 1;
+  a.idle_ns = (u64)(st->idle_timeout_s * 1e9);
+  a.n_jobs = 0;
+  *(volatile int*)s->h_stop = 0;
+  int grid = 0;
+  int rc = launch_batch(s, a, (long long)s->lanes, st->kstream, &grid);
+  if (rc) return rc;
+  CUDA_TRY(cudaEventRecord(st->kdone, st->kstream));
+  st->launched = true;
+  st->launches++;
+  return DDG_OK;
+}
+
+int ddg_stream_open(ddg_solver* s, int ring_slots, double idle_timeout_s, ddg_stream** out) {
+  if (!out) return fail(DDG_E_ARG, "null output");
+  *out = nullptr;
+  if (!s) return fail(DDG_E_ARG, "null solver");
+  if (s->streaming) return fail(DDG_E_STATE, "a stream is already open on this solver");
+  if (s->cfg.schedule != 0) return fail(DDG_E_ARG, "streams run on the block-phase kernel (schedule 0)");
+  if (ring_slots <= 0) ring_slots = 65536;
+  if (ring_slots < 64 || ring_slots > (1 << 22) || (ring_slots & (ring_slots - 1)))
+    return fail(DDG_E_ARG, "ring_slots %d is not a power of two in 64..4M", ring_slots);
+  CUDA_TRY(cudaSetDevice(s->device));
+  ddg_stream* st = new ddg_stream();
+  st->s = s;
+  st->slots = ring_slots;
+  st->idle_timeout_s = idle_timeout_s > 0 ? idle_timeout_s : 30;
+  // Admission by TT memory: a deal's jobs each need a lane (and its TT); at most two jobs
+  // per lane are admitted, one running and one waiting.
+  st->admit = (long long)s->lanes * 2 / s->cfg.jobs_per_deal;
+  if (st->admit > ring_slots) st->admit = ring_slots;
+  if (st->admit < 1) st->admit = 1;
+  st->slot_busy.assign(ring_slots, 0);
+  s->streaming = true;
+  cudaError_t e = cudaMalloc(&st->d_ring, (size_t)ring_slots * 32);
+  if (e == cudaSuccess) e = cudaMalloc(&st->d_out, (size_t)ring_slots * 20);
+  if (e == cudaSuccess) e = cudaMalloc(&st->d_done, (size_t)ring_slots * 4);
+  if (e == cudaSuccess) e = cudaMalloc(&st->d_words, 4 * 8);
+  if (e == cudaSuccess) e = cudaHostAlloc(&st->h_comp, (size_t)ring_slots * sizeof(CompRec), cudaHostAllocMapped);
+  if (e == cudaSuccess) e = cudaHostGetDevicePointer((void**)&st->d_comp, st->h_comp, 0);
+  if (e == cudaSuccess) e = cudaHostAlloc(&st->h_stage, (size_t)ring_slots * 32, cudaHostAllocDefault);
+  if (e == cudaSuccess) e = cudaHostAlloc(&st->h_words, 4 * 8, cudaHostAllocDefault);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&st->kstream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&st->cstream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&st->kdone, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaMemset(st->d_done, 0, (size_t)ring_slots * 4);
+  if (e == cudaSuccess) e = cudaMemset(st->d_words, 0, 4 * 8);
+  if (e == cudaSuccess) e = cudaMemset(s->counters, 0, CNT_WORDS * 8);
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) {
+    stream_free(st);
+    return fail(e == cudaErrorMemoryAllocation ? DDG_E_MEMORY : DDG_E_CUDA, "stream buffers: %s",
+                cudaGetErrorString(e));
+  }
+  memset(st->h_comp, 0, (size_t)ring_slots * sizeof(CompRec));
+  int rc = stream_kernel(st);
+  if (rc) {
+    stream_free(st);
+    return rc;
+  }
+  *out = st;
+  return DDG_OK;
+}
+
+int64_t ddg_stream_capacity(const ddg_stream* st) { return st ? st->admit : 0; }
+int64_t ddg_stream_in_flight(const ddg_stream* st) { return st ? (int64_t)(st->published - st->consumed) : 0; }
+
+int ddg_stream_submit(ddg_stream* st, const uint64_t* hands, int64_t n, int64_t* accepted) {
+  if (accepted) *accepted = 0;
+  if (!st) return fail(DDG_E_ARG, "null stream");
+  if (n < 0 || (n > 0 && !hands)) return fail(DDG_E_ARG, "bad submit arguments");
+  for (int64_t i = 0; i < n; i++) {
+    int rc = ddg_check_deal(hands + i * 4);
+    if (rc) return fail(rc, "deal %lld: %s", (long long)i, g_err);
+  }
+  CUDA_TRY(cudaSetDevice(st->s->device));
+  const unsigned long long mask = (unsigned long long)st->slots - 1;
+  // Admission: ring slots and TT memory; a slot is reused only after its deal was polled.
+  int64_t k = 0;
+  while (k < n && (long long)(st->published + k - st->consumed) < st->admit &&
+         !st->slot_busy[(st->published + k) & mask])
+    k++;
+  if (k > 0) {
+    const unsigned long long first = st->published & mask;
+    for (int64_t i = 0; i < k; i++) {
+      const unsigned long long slot = (st->published + i) & mask;
+      memcpy(st->h_stage + slot * 4, hands + i * 4, 32);
+      st->slot_busy[slot] = 1;
     }
-    st->jobs_done = (int64_t)c[CNT_JOBS_DONE];
-    float ms = 0;
-    CUDA_TRY(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
-    st->kernel_ms = ms;
-    st->grid = grid;
-    st->block = s->block;
-    st->lanes = grid * s->block;
+    const unsigned long long run1 = std::min<unsigned long long>((unsigned long long)k, st->slots - first);
+    CUDA_TRY(cudaMemcpyAsync(st->d_ring + first * 4, st->h_stage + first * 4, run1 * 32, cudaMemcpyHostToDevice,
+                             st->cstream));
+    if ((unsigned long long)k > run1)
+      CUDA_TRY(cudaMemcpyAsync(st->d_ring, st->h_stage, (k - run1) * 32, cudaMemcpyHostToDevice, st->cstream));
+    st->h_words[0] = st->published + k;  // published after the deals (same copy stream)
+    CUDA_TRY(cudaMemcpyAsync(st->d_words + 0, st->h_words + 0, 8, cudaMemcpyHostToDevice, st->cstream));
+    CUDA_TRY(cudaStreamSynchronize(st->cstream));
+    st->published += k;
+  }
+  if (accepted) *accepted = k;
+  return stream_kernel(st);
+}
+
+int ddg_stream_poll(ddg_stream* st, uint8_t* rec28, int64_t max, int64_t* got) {
+  if (got) *got = 0;
+  if (!st) return fail(DDG_E_ARG, "null stream");
+  if (max < 0 || (max > 0 && !rec28)) return fail(DDG_E_ARG, "bad poll arguments");
+  const unsigned long long mask = (unsigned long long)st->slots - 1;
+  int64_t k = 0;
+  while (k < max) {
+    volatile CompRec* r = st->h_comp + (st->consumed & mask);
+    if (r->flag != (unsigned)(st->consumed + 1)) break;
+    std::atomic_thread_fence(std::memory_order_acquire);
+    const unsigned long long seq = r->seq;
+    memcpy(rec28 + k * 28, &seq, 8);
+    for (int b = 0; b < 20; b++) rec28[k * 28 + 8 + b] = r->tricks[b];
+    st->slot_busy[seq & mask] = 0;
+    st->consumed++;
+    k++;
+  }
+  if (got) *got = k;
+  if (st->published > st->consumed) {
+    CUDA_TRY(cudaSetDevice(st->s->device));
+    return stream_kernel(st);  // lanes that timed out come back for work still in flight
   }
   return DDG_OK;
+}
+
+int ddg_stream_close(ddg_stream* st, int drain, ddg_stats* stats) {
+  if (!st) return fail(DDG_E_ARG, "null stream");
+  if (stats) memset(stats, 0, sizeof(*stats));
+  cudaSetDevice(st->s->device);
+  if (!drain) *(volatile int*)st->s->h_stop = 1;  // blocks end at their next check
+  st->h_words[3] = 1;  // closing: lanes end once every published deal is taken and done
+  cudaError_t e = cudaMemcpyAsync(st->d_words + 3, st->h_words + 3, 8, cudaMemcpyHostToDevice, st->cstream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st->cstream);
+  int rc = e == cudaSuccess ? DDG_OK : fail(DDG_E_CUDA, "stream close: %s", cudaGetErrorString(e));
+  // The kernel ends when its lanes find nothing left; if it had timed out with work left,
+  // one more launch finishes it.
+  for (int round = 0; rc == DDG_OK && round < 2; round++) {
+    e = cudaEventSynchronize(st->kdone);
+    if (e != cudaSuccess) {
+      rc = fail(DDG_E_CUDA, "stream kernel: %s", cudaGetErrorString(e));
+      break;
+    }
+    st->launched = false;
+    unsigned long long words[4];
+    e = cudaMemcpy(words, st->d_words, sizeof(words), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) {
+      rc = fail(DDG_E_CUDA, "stream close: %s", cudaGetErrorString(e));
+      break;
+    }
+    if (!drain || words[2] >= st->published) break;
+    rc = stream_kernel(st);
+  }
+  if (rc == DDG_OK && stats) {
+    unsigned long long c[CNT_WORDS];
+    e = cudaMemcpy(c, st->s->counters, sizeof(c), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) {
+      stats->nodes = c[CNT_NODES];
+      stats->tt_probes = c[CNT_PROBES];
+      stats->tt_hits = c[CNT_HITS];
+      stats->tt_stores = c[CNT_STORES];
+      stats->tt_bytes = c[CNT_TT_BYTES];
+      for (int k = 0; k < 7; k++) stats->enter_exit[k] = c[CNT_EXIT + k];
+      stats->jobs_done = (int64_t)c[CNT_JOBS_DONE];
+      stats->iterations = c[CNT_ITERS];
+      stats->lanes = st->s->lanes;
+      stats->block = st->s->block;
+      stats->grid = st->s->lanes / st->s->block;
+      stats->tasks = (uint64_t)st->launches;
+    }
+    st->s->total_nodes += c[CNT_NODES];
+  }
+  stream_free(st);
+  return rc;
 }
 
 static int ensure_staging(ddg_solver* s, int64_t n) {

@@ -35,6 +35,7 @@ enum {
   CNT_TASKS = 31,         // tasks donated to helpers
   CNT_PHASE_CYCLES = 32,  // 8 words: SM cycles per phase, summed over blocks
   CNT_FAULTS = 38,        // blocks whose bounded queue wait gave up (never expected)
+  CNT_BLOCKS_DONE = 39,   // blocks that ended with every lane idle (the solve is complete)
   CNT_WORDS = 40
 };
 
@@ -57,7 +58,29 @@ struct BatchArgs {
   TaskPool* tasks;       // helping: idle lanes take donated moves (tricks exact), or null
   int free_below;        // fewer busy lanes than this in a block: each thread runs its own lane
   int free_steps;        // stages a lane runs per free-running round
+  struct LaneSave* save; // resumable solve: lane states kept between launches, or null
+  int resume;            // 1: lanes start from `save` (a later slice of the same solve)
+  u64 slice_ns;          // resumable solve: each block stops this long after it starts (0 = never)
+  unsigned long long* next_job;  // job queue head (counters + CNT_NEXT_JOB, or the stream's)
+  // Stream mode (ring != null): deals come from a device ring the host keeps filling.
+  const u64* ring;                         // slots * 4 hands; deal seq lives in slot seq & ring_mask
+  const unsigned long long* published;     // deals published so far (device word, host-written)
+  const int* closing;                      // 1: no deal will be published any more
+  int* deal_done;                          // per slot: jobs of the deal finished
+  struct CompRec* comp;                    // completion records (mapped host memory), slots of them
+  unsigned long long* comp_tail;           // completion records written so far
+  long long ring_mask;
+  u64 idle_ns;                             // a block whose lanes found no deal this long ends
 };
+
+// One finished deal of a stream: its sequence number and table; `flag` = record index + 1,
+// written last, tells the host the record is complete.
+struct CompRec {
+  unsigned long long seq;
+  uint8_t tricks[20];
+  unsigned flag;
+};
+static_assert(sizeof(CompRec) == 32, "completion record is 32 bytes");
 
 __device__ __forceinline__ u64 global_ns() {
   u64 t;
@@ -71,6 +94,49 @@ struct LaneCounters {
   u64 tt_key;  // (deal, strain) key of the helper tasks the lane's TT holds, 0 = none
   u32 jobs_done;
 };
+
+// A lane between two slices of a resumable solve (HBM): its whole search state, the nodes
+// its current job or task has taken so far, and its TT key.
+struct LaneSave {
+  Lane L;
+  u64 progress;
+  u64 tt_key;
+};
+
+// Start of a launch: a fresh lane, or the lane as the previous slice left it.
+__device__ __forceinline__ void lane_begin(const BatchArgs& a, long long lane, Lane& L, LaneCounters& c) {
+  memset(&c, 0, sizeof(LaneCounters));
+  if (a.resume) {
+    const LaneSave& sv = a.save[lane];
+    L = sv.L;
+    c.start_nodes = 0ull - sv.progress;  // work_nodes() = progress + this slice's nodes
+    c.tt_key = sv.tt_key;
+    return;
+  }
+  L.stage = ST_TAKE;
+  L.sp = 0;
+  L.gen = a.lane_gen[lane];
+  L.v = 0;
+  L.r = 0;
+  L.p.trick = 0;
+  L.task = -1;
+}
+
+// End of a launch: the TT generation, and for a resumable solve the lane's state.
+__device__ __forceinline__ void lane_end(const BatchArgs& a, long long lane, const Lane& L, const LaneCounters& c) {
+  a.lane_gen[lane] = L.gen;
+  if (a.save) {
+    LaneSave& sv = a.save[lane];
+    sv.L = L;
+    sv.progress = c.s.nodes - c.start_nodes;
+    sv.tt_key = c.tt_key;
+  }
+}
+
+// The block's stop test (thread 0): the host's flag, or the end of the slice.
+__device__ __forceinline__ bool stop_requested(const BatchArgs& a, u64 t_end) {
+  return (a.stop && *a.stop) || (t_end && global_ns() > t_end);
+}
 
 struct DevEnv {
   const BatchArgs* a;
@@ -96,13 +162,24 @@ struct DevEnv {
   __device__ __forceinline__ u64 work_nodes() { return c->s.nodes - c->start_nodes; }
   __device__ __forceinline__ void task_started() { c->start_nodes = c->s.nodes; }
   __device__ __forceinline__ u64& tt_key() { return c->tt_key; }
-  __device__ __forceinline__ bool take(Lane& L) {
-    unsigned long long job = atomicAdd(a->counters + CNT_NEXT_JOB, 1ull);
-    if ((long long)job >= a->n_jobs) return false;
-    L.job = (long long)job;
-    L.deal = L.job / a->jpd;
+  // 1: a job; 0: no job will come; -1 (stream): none published yet.
+  __device__ __forceinline__ int take(Lane& L) {
+    unsigned long long job;
+    const u64* hands;
+    if (a->ring) {
+      if (!stream_take(job)) return *reinterpret_cast<const volatile int*>(a->closing) && !stream_more() ? 0 : -1;
+      L.job = (long long)job;
+      L.deal = L.job / a->jpd;
+      hands = a->ring + (L.deal & a->ring_mask) * 4;
+    } else {
+      job = atomicAdd(a->next_job, 1ull);
+      if ((long long)job >= a->n_jobs) return 0;
+      L.job = (long long)job;
+      L.deal = L.job / a->jpd;
+      hands = a->hands + L.deal * 4;
+    }
     int sub = (int)(L.job - L.deal * a->jpd);
-    const ulonglong2* h = reinterpret_cast<const ulonglong2*>(a->hands + L.deal * 4);
+    const ulonglong2* h = reinterpret_cast<const ulonglong2*>(hands);
     ulonglong2 x = h[0], y = h[1];
     L.p.h[0] = x.x;
     L.p.h[1] = x.y;
@@ -119,18 +196,58 @@ struct DevEnv {
     }
     L.mode = a->mode;
     c->start_nodes = c->s.nodes;
-    return true;
+    return 1;
+  }
+  // Stream: claims the next published job, if any.
+  __device__ __forceinline__ bool stream_take(unsigned long long& job) {
+    const long long avail = (long long)*reinterpret_cast<const volatile unsigned long long*>(a->published) * a->jpd;
+    unsigned long long j = *reinterpret_cast<volatile unsigned long long*>(a->next_job);
+    for (int tries = 0; tries < 8; tries++) {
+      if ((long long)j >= avail) return false;
+      const unsigned long long prev = atomicCAS(a->next_job, j, j + 1);
+      if (prev == j) {
+        job = j;
+        return true;
+      }
+      j = prev;
+    }
+    return false;
+  }
+  // Stream, after `closing` was seen: were deals published that no lane has taken yet?
+  __device__ __forceinline__ bool stream_more() {
+    __threadfence();
+    const long long avail = (long long)*reinterpret_cast<const volatile unsigned long long*>(a->published) * a->jpd;
+    return (long long)*reinterpret_cast<volatile unsigned long long*>(a->next_job) < avail;
   }
   __device__ __forceinline__ int seed(const Lane& L) {
     return a->mode == MODE_STEP ? (int)a->seeds[L.deal * 20 + L.strain * 4 + L.decl] : 7;
   }
+  __device__ __forceinline__ long long out_row(const Lane& L) const {
+    return a->ring ? (L.deal & a->ring_mask) : L.deal;
+  }
   __device__ __forceinline__ void answer(const Lane& L, int ns) {
-    a->out20[L.deal * 20 + L.strain * 4 + L.decl] = (uint8_t)((L.decl & 1) == 0 ? ns : 13 - ns);
+    a->out20[out_row(L) * 20 + L.strain * 4 + L.decl] = (uint8_t)((L.decl & 1) == 0 ? ns : 13 - ns);
   }
   __device__ __forceinline__ void job_done(const Lane& L) {
     if (a->job_nodes) a->job_nodes[L.job] = c->s.nodes - c->start_nodes;
     if (a->job_end_ns) a->job_end_ns[L.job] = global_ns();
     c->jobs_done++;
+    if (a->ring) stream_job_done(L);
+  }
+  // Stream: the lane that finishes a deal's last job writes its completion record.
+  __device__ __noinline__ void stream_job_done(const Lane& L) {
+    const long long slot = L.deal & a->ring_mask;
+    __threadfence();  // this job's answers before the count
+    if (atomicAdd(a->deal_done + slot, 1) != a->jpd - 1) return;
+    __threadfence();  // every job's answers are visible now
+    const volatile uint8_t* o = a->out20 + slot * 20;
+    const unsigned long long idx = atomicAdd(a->comp_tail, 1ull);
+    volatile CompRec* r = a->comp + (idx & (unsigned long long)a->ring_mask);
+    r->seq = (unsigned long long)L.deal;
+    for (int k = 0; k < 20; k++) r->tricks[k] = o[k];
+    __threadfence_system();  // the record before its flag
+    r->flag = (unsigned)idx + 1u;
+    a->deal_done[slot] = 0;
   }
 };
 
@@ -156,6 +273,8 @@ struct BlockShared {
   unsigned parked[BLOCK / 32];  // lanes waiting on the task pool (HUNGRY, WAIT)
   int live;                     // lanes not IDLE
   int fault;                    // a queue slot was never written (bounded wait gave up)
+  u64 idle_since;               // stream: global time since which no lane had work (0 = busy)
+  int idle_exit;                // stream: waiting lanes end
 };
 
 // Position of the r-th (0-based) set bit of m (r < popc(m)).
@@ -252,17 +371,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(BatchArgs a) {
   BlockShared<BLOCK>& sh = *reinterpret_cast<BlockShared<BLOCK>*>(smem_raw);
   const int tid = threadIdx.x;
   const long long base = (long long)blockIdx.x * BLOCK;
-  memset(&sh.cnt[tid], 0, sizeof(LaneCounters));
-  {
-    Lane& L = sh.lane[tid];
-    L.stage = ST_TAKE;
-    L.sp = 0;
-    L.gen = a.lane_gen[base + tid];
-    L.v = 0;
-    L.r = 0;
-    L.p.trick = 0;
-    L.task = -1;
-  }
+  lane_begin(a, base + tid, sh.lane[tid], sh.cnt[tid]);
+  const u64 t_end = a.slice_ns ? global_ns() + a.slice_ns : 0;
   if (tid < PH_COUNT) {
     sh.ph_warps[tid] = 0;
     sh.ph_items[tid] = 0;
@@ -277,13 +387,16 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(BatchArgs a) {
     sh.all_done = 0;
     sh.free_rounds = 0;
     sh.free_cycles = 0;
+    sh.idle_since = 0;
+    sh.idle_exit = 0;
   }
   __syncthreads();
   for (unsigned iter = 0;; iter++) {
-    if (tid == 0 && a.stop && (iter & 63u) == 63u && *a.stop) sh.stop = 1;
+    if (tid == 0 && (iter & 15u) == 15u && stop_requested(a, t_end)) sh.stop = 1;
     if (!__syncthreads_or(sh.lane[tid].stage != ST_IDLE)) break;
-    if (sh.stop) {  // host time limit: unfinished results stay 255
-      sh.lane[tid].stage = ST_IDLE;
+    if (sh.stop) {
+      if (a.save) break;  // resumable: the lanes are kept for the next slice
+      sh.lane[tid].stage = ST_IDLE;  // host time limit: unfinished results stay 255
       continue;
     }
     if (tid == 0) {
@@ -295,8 +408,26 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(BatchArgs a) {
         sh.all_done = atom_load(&a.tasks->exhausted) && atom_load(&a.tasks->busy) == 0;
       }
     }
-    const int st0 = sh.lane[tid].stage;
-    const int busy_here = __syncthreads_count(st0 != ST_HUNGRY && st0 != ST_IDLE);
+    int st0 = sh.lane[tid].stage;
+    int busy_here = __syncthreads_count(st0 != ST_HUNGRY && st0 != ST_IDLE);
+    if (a.ring) {
+      // Stream: lanes waiting for a deal (TAKE) are not work. A block with nothing to do
+      // naps between polls of the ring, and after idle_ns without work its waiting lanes
+      // end (the host launches the kernel again when it publishes more).
+      busy_here = __syncthreads_count(st0 != ST_HUNGRY && st0 != ST_IDLE && st0 != ST_TAKE);
+      if (busy_here == 0) {
+        if (tid == 0) {
+          const u64 now = global_ns();
+          if (!sh.idle_since) sh.idle_since = now;
+          else if (now - sh.idle_since > a.idle_ns) sh.idle_exit = 1;
+        }
+        __nanosleep(20000);
+      } else if (tid == 0) {
+        sh.idle_since = 0;
+      }
+      __syncthreads();
+      if (sh.idle_exit && st0 == ST_TAKE) sh.lane[tid].stage = ST_IDLE;
+    }
     if (busy_here < a.free_below) {
       // Few busy lanes: each thread runs its own lane for a while, no phases.
       const long long f0 = clock64();
@@ -336,8 +467,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(BatchArgs a) {
       sh.ph_cycles[PH_MOVES_FOLLOW] += t5 - t4;
     }
   }
-  a.lane_gen[base + tid] = sh.lane[tid].gen;
-  __syncthreads();
+  lane_end(a, base + tid, sh.lane[tid], sh.cnt[tid]);
+  const int busy_left = __syncthreads_or(sh.lane[tid].stage != ST_IDLE);
+  if (tid == 0 && !busy_left) atomicAdd(a.counters + CNT_BLOCKS_DONE, 1ull);
   block_counters(sh, a, tid);
 }
 
@@ -386,25 +518,15 @@ __global__ void __launch_bounds__(BLOCK, MINB) queue_kernel(BatchArgs a) {
   BlockShared<BLOCK>& sh = *reinterpret_cast<BlockShared<BLOCK>*>(smem_raw);
   const int tid = threadIdx.x, ln = tid & 31;
   const long long base = (long long)blockIdx.x * BLOCK;
-  memset(&sh.cnt[tid], 0, sizeof(LaneCounters));
-  {
-    Lane& L = sh.lane[tid];
-    L.stage = ST_TAKE;
-    L.sp = 0;
-    L.gen = a.lane_gen[base + tid];
-    L.v = 0;
-    L.r = 0;
-    L.p.trick = 0;
-    L.task = -1;
-    sh.q[PH_CHEAP][tid] = (uint16_t)(tid + 1);
-    for (int p = 1; p < PH_COUNT; p++) sh.q[p][tid] = 0;
-  }
+  lane_begin(a, base + tid, sh.lane[tid], sh.cnt[tid]);
+  const u64 t_end = a.slice_ns ? global_ns() + a.slice_ns : 0;
+  for (int p = 0; p < PH_COUNT; p++) sh.q[p][tid] = 0;
   if (tid < PH_COUNT) {
     sh.ph_warps[tid] = 0;
     sh.ph_items[tid] = 0;
     sh.ph_cycles[tid] = 0;
     sh.qhead[tid] = 0;
-    sh.qtail[tid] = tid == PH_CHEAP ? BLOCK : 0;
+    sh.qtail[tid] = 0;
   }
   if (tid < BLOCK / 32) sh.parked[tid] = 0;
   if (tid == 0) {
@@ -416,9 +538,12 @@ __global__ void __launch_bounds__(BLOCK, MINB) queue_kernel(BatchArgs a) {
     sh.all_done = 0;
     sh.free_rounds = 0;
     sh.free_cycles = 0;
-    sh.live = BLOCK;
+    sh.live = 0;
     sh.fault = 0;
   }
+  __syncthreads();
+  route_lane(sh, sh.lane[tid].stage != ST_IDLE, tid, ln);  // every lane to its first queue
+  if (sh.lane[tid].stage != ST_IDLE) atomicAdd(&sh.live, 1);
   __syncthreads();
   volatile unsigned* vhead = sh.qhead;
   volatile unsigned* vtail = sh.qtail;
@@ -428,7 +553,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) queue_kernel(BatchArgs a) {
   unsigned poll_word = (unsigned)(tid >> 5);
   for (unsigned loop = 0;; loop++) {
     if (__shfl_sync(0xFFFFFFFFu, (*vstop | *vfault), 0)) break;  // warp-uniform
-    if (ln == 0 && (loop & 63u) == 63u && a.stop && *a.stop) sh.stop = 1;
+    if (ln == 0 && (loop & 63u) == 63u && stop_requested(a, t_end)) sh.stop = 1;
     if (a.tasks && ln == 0 && (loop & 15u) == 0) {
       const int q = atom_load(&a.tasks->queued), h = atom_load(&a.tasks->hungry);
       sh.help_hint = h > q;
@@ -536,8 +661,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) queue_kernel(BatchArgs a) {
     }
   }
   __syncthreads();
-  a.lane_gen[base + tid] = sh.lane[tid].gen;
+  lane_end(a, base + tid, sh.lane[tid], sh.cnt[tid]);
   if (tid == 0 && sh.fault) atomicAdd(a.counters + CNT_FAULTS, 1ull);
+  if (tid == 0 && sh.live == 0) atomicAdd(a.counters + CNT_BLOCKS_DONE, 1ull);
   __syncthreads();
   block_counters(sh, a, tid);
 }
@@ -566,7 +692,7 @@ __device__ __forceinline__ void block_counters(BlockShared<BLOCK>& sh, const Bat
     if (tid >= CNT_PHASE_CYCLES && tid < CNT_PHASE_CYCLES + PH_COUNT) sum = sh.ph_cycles[tid - CNT_PHASE_CYCLES];
     if (tid == CNT_PHASE_CYCLES + PH_COUNT) sum = sh.free_cycles;
     if (tid == CNT_PHASE_ITEMS + PH_COUNT) sum = sh.free_rounds;
-    if (tid != CNT_NEXT_JOB && sum) atomicAdd(a.counters + tid, sum);
+    if (tid != CNT_NEXT_JOB && tid != CNT_FAULTS && tid != CNT_BLOCKS_DONE && sum) atomicAdd(a.counters + tid, sum);
   }
 }
 

@@ -668,7 +668,12 @@ DDG_CALL void node_done(Lane& L, Env& env) {
 template <class Env>
 DDG_CALL void step_take(Lane& L, Env& env) {
   TaskPool* tp = env.pool();
-  if (!env.take(L)) {
+  const int got = env.take(L);
+  if (got < 0) {  // a stream with no deal published yet: try again later
+    L.stage = ST_TAKE;
+    return;
+  }
+  if (!got) {
     if (tp) {
       tp->exhausted = 1;
       atom_add(&tp->hungry, 1);
@@ -973,7 +978,10 @@ DDG_CALL void advance_cheap(Lane& L, Env& env) {
         step_next(L, env);
         break;
       case ST_ROOT: step_root(L, env); break;
-      case ST_TAKE: step_take(L, env); break;
+      case ST_TAKE:
+        step_take(L, env);
+        if (L.stage == ST_TAKE) return;  // nothing to take yet
+        break;
       case ST_WAIT:
         if (!step_wait(L, env)) return;
         break;
@@ -1009,7 +1017,10 @@ DDG_CALL void advance_free(Lane& L, Env& env, int max_steps, bool may_claim) {
         }
         step_next(L, env);
         break;
-      case ST_TAKE: step_take(L, env); break;
+      case ST_TAKE:
+        step_take(L, env);
+        if (L.stage == ST_TAKE) return;
+        break;
       case ST_ROOT: step_root(L, env); break;
       case ST_ENTER: step_enter(L, env); break;
       case ST_MOVES_LEAD:

@@ -121,6 +121,46 @@ int ddg_solve_batch_seeded(ddg_solver* s, const uint64_t* hands, int64_t n, cons
 int ddg_solve_device(ddg_solver* s, const uint64_t* d_hands, int64_t n, const int8_t* d_seed20,
                      uint8_t* d_out20, uint64_t* d_job_nodes, void* stream, ddg_stats* st);
 
+/* Resumable (time-sliced) solve of n deals on device buffers. ddg_solve_begin sets it up
+ * (results = 255 until solved); each ddg_solve_continue runs it for at most `seconds` and
+ * returns with every lane's search state kept in device memory, so the next call goes on
+ * where this one stopped; *finished = 1 once every result is written. `hands_host`
+ * (n*4 uint64, pinned for an asynchronous copy) is copied over d_hands before the slice
+ * and `out20_host` (n*20) receives d_out20 after it, when not NULL. st = this slice's
+ * counters (jobs_done = jobs finished in the slice). The reference's TIME_LIMIT
+ * (gpu/gpu_main.cu:247-266) ends its kernel and drops unfinished jobs; a slice keeps them.
+ * Another solve call on the same solver ends a resumable solve. */
+int ddg_solve_begin(ddg_solver* s, const uint64_t* d_hands, int64_t n, const int8_t* d_seed20,
+                    uint8_t* d_out20, void* stream);
+int ddg_solve_continue(ddg_solver* s, double seconds, const uint64_t* hands_host, uint8_t* out20_host,
+                       void* stream, ddg_stats* st, int* finished);
+
+/* Streams (continuous batching; the reference's dd_stream, gpu/stream_main.cu:38-114,
+ * 189-332). A stream keeps the solver's lanes running as one persistent kernel that takes
+ * jobs from a device-resident ring of deals while the host keeps publishing new ones; a
+ * deal's 28-byte record (uint64 0-based submission index, then tricks[strain][declarer],
+ * gpu/stream_main.cu:298-302) is available as soon as its last job ends, out of order.
+ * ring_slots: power of two, 64..4M (0 = 65,536). Admission: ddg_stream_submit accepts
+ * deals only while ring slots are free and at most 2 * lanes jobs are in flight (each job
+ * holds a lane and its TT); *accepted says how many of the n it took, in order. Deals wait
+ * for nothing but a free lane: requests that arrive while others are on the GPU start as
+ * lanes free up. Lanes that find no deal for idle_timeout_s (0 = 30 s) end; the next
+ * submit or poll launches the kernel again. While a stream is open the solver's other
+ * calls return DDG_E_STATE. Runs on the block-phase kernel (schedule 0), helping off. */
+typedef struct ddg_stream ddg_stream;
+int ddg_stream_open(ddg_solver* s, int ring_slots, double idle_timeout_s, ddg_stream** out);
+int ddg_stream_submit(ddg_stream* st, const uint64_t* hands, int64_t n, int64_t* accepted);
+/* Copies up to `max` finished deals' 28-byte records into rec28; *got = how many. */
+int ddg_stream_poll(ddg_stream* st, uint8_t* rec28, int64_t max, int64_t* got);
+/* Deals submitted and not yet polled; the admission limit on them. */
+int64_t ddg_stream_in_flight(const ddg_stream* st);
+int64_t ddg_stream_capacity(const ddg_stream* st);
+/* Ends the stream: drain = 1 waits until every submitted deal is solved, 0 stops the
+ * lanes at once (deals in flight are dropped, as the reference's bench stop,
+ * gpu/stream_main.cu:320-323). Records not polled are dropped. st_out = counters over the
+ * stream's life (tasks = kernel launches). Frees the stream. */
+int ddg_stream_close(ddg_stream* st, int drain, ddg_stats* st_out);
+
 /* One strain of one deal, declarers N,E,S,W (tricks as ints): the reference's
  * dd_solve_strain (src/dd.h:926) and dd_solve_strain_guess (src/dd.h:915; ns4 = NS seeds,
  * NULL = binary search). For many deals use ddg_solve_batch. */

@@ -16,6 +16,10 @@ g++ -O3 -std=c++17 -march=x86-64-v3 -pthread -fPIC -shared -I"$REF_DIR/src" \
   -o "$OUT/libddref.so.tmp" "$HERE/ref_shim.cpp"
 mv "$OUT/libddref.so.tmp" "$OUT/libddref.so"
 echo "built $OUT/libddref.so"
+g++ -O3 -std=c++17 -march=x86-64-v3 -pthread -DWITH_REF -I"$REF_DIR/src" \
+  -o "$OUT/cpu_window.tmp" "$HERE/cpu_window.cpp"
+mv "$OUT/cpu_window.tmp" "$OUT/cpu_window"
+echo "built $OUT/cpu_window"
 # The reference's own GPU batch driver (gpu/gpu_main.cu), for sm_100a: a timing baseline
 # of its wavefront kernel on the same GPU (run with WAVE=1 and CHECK=0).
 if command -v nvcc > /dev/null && [ -f "$REF_DIR/gpu/gpu_main.cu" ]; then

@@ -1477,6 +1477,23 @@ long long ddo_solve_batch(const uint64_t* hands, long n, int tt_log2, int thread
   return (long long)b.nodes;
 }
 
+/* One (deal, strain) job at a time on a caller-held context (one TT), as the reference's
+ * dd_solve_strain on a DDCtx (src/dd.h:926-939): returns the job's nodes. */
+void* ddo_ctx_new(int tt_log2) {
+  if (tt_log2 < 9 || tt_log2 > 24) return NULL;
+  return solver_new(tt_log2);
+}
+long long ddo_ctx_solve_strain(void* ctx, const uint64_t* hands4, int strain, int* out4) {
+  OSolver* s = (OSolver*)ctx;
+  if (!s || strain < 0 || strain > 4) return -1;
+  u64 before = s->c.nodes;
+  solve_job(&s->c, hands4, strain, 0, 3, NULL, out4);
+  return (long long)(s->c.nodes - before);
+}
+void ddo_ctx_free(void* ctx) {
+  if (ctx) solver_free((OSolver*)ctx);
+}
+
 /* Unpruned minimax: NS tricks from the position with `leader` to lead (the reference's
  * brute force of tests/test_small.cpp:11-46, for small endings). */
 static int brute_rec(OCtx* c) {

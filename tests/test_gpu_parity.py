@@ -149,3 +149,95 @@ def test_helping_splits_hard_deals(ddg, helper_solver):
     t, _, st = device_solve(ddg, helper_solver, hands)
     assert (t == g["tricks"][LIGHT_13]).all()
     assert st["tasks"] > 0
+
+
+@pytest.mark.parametrize("schedule", [0, 1])
+def test_resumable_slices(ddg, schedule):
+    """A solve cut into short slices (lane states kept in HBM between launches) gives the
+    reference's tricks and exactly the node counts of one uninterrupted solve."""
+    import torch
+    g = load_golden("k8_120.npz")
+    n = g["hands"].shape[0]
+    s = ddg.Solver(tt_log2=10, jobs_per_deal=5, lanes=2048, block=256, min_blocks=2, schedule=schedule)
+    try:
+        d_h = torch.from_numpy(g["hands"].view(np.int64)).cuda()
+        d_o = torch.empty(n * 20, dtype=torch.uint8, device="cuda")
+        s.begin(d_h.data_ptr(), n, d_o.data_ptr())
+        nodes = jobs = slices = 0
+        finished = False
+        while not finished:
+            finished, st = s.resume(0.002)
+            nodes += st["nodes"]
+            jobs += st["jobs_done"]
+            slices += 1
+            assert slices < 100000
+        assert slices > 2
+        assert (d_o.cpu().numpy().reshape(n, 5, 4) == g["tricks"]).all()
+        assert nodes == int(g["nodes_jpd5"].astype(np.int64).sum())
+        assert jobs == n * 5
+        # a finished solve stays finished; a plain solve afterwards works as before
+        assert s.resume(0.002)[0]
+        t, _, _ = device_solve(ddg, s, g["hands"])
+        assert (t == g["tricks"]).all()
+    finally:
+        s.close()
+
+
+def test_queue_kernel_parity(ddg):
+    """The barrier-free queue kernel (schedule 1) runs the same stages: same tricks and
+    node counts as the reference."""
+    g = load_golden("k6_4096.npz")
+    s = ddg.Solver(tt_log2=10, jobs_per_deal=5, block=256, min_blocks=2, schedule=1)
+    try:
+        t, nodes, st = device_solve(ddg, s, g["hands"])
+        assert (t == g["tricks"]).all()
+        assert (nodes == g["nodes_jpd5"]).all()
+    finally:
+        s.close()
+
+
+def test_stream_continuous_batching(ddg):
+    """Deals submitted while others are on the GPU come back with the same tables as when
+    each is solved alone (and as the reference's), out of order, each exactly once."""
+    import time
+    g = load_golden("k7_120.npz")
+    hands, want = g["hands"], g["tricks"]
+    s = ddg.Solver(tt_log2=10, jobs_per_deal=5, lanes=4096, block=256, min_blocks=2)
+    try:
+        # alone: one deal at a time
+        st = ddg.Stream(s, ring_slots=64, idle_timeout_s=5)
+        alone = np.zeros_like(want)
+        for i in range(8):
+            assert st.submit(hands[i:i + 1]) == 1
+            t0 = time.time()
+            while True:
+                idx, tab = st.poll()
+                if len(idx):
+                    assert list(idx) == [i]
+                    alone[i] = tab[0]
+                    break
+                assert time.time() - t0 < 60
+        st.close()
+        # in the mix: everything at once through a small ring (admission holds the rest back)
+        st = ddg.Stream(s, ring_slots=64, idle_timeout_s=5)
+        got = np.full_like(want, 255)
+        seen = np.zeros(len(hands), dtype=int)
+        sent = 0
+        t0 = time.time()
+        while seen.sum() < len(hands):
+            if sent < len(hands):
+                sent += st.submit(hands[sent:])
+            idx, tab = st.poll()
+            for k, i in enumerate(idx):
+                seen[i] += 1
+                got[i] = tab[k]
+            assert time.time() - t0 < 120
+        stats = st.close()
+        assert (seen == 1).all()
+        assert (got == want).all()
+        assert (alone[:8] == got[:8]).all()
+        assert stats["jobs_done"] == len(hands) * 5
+        # the solver works normally after the stream is closed
+        assert (s.solve(hands[:4]) == want[:4]).all()
+    finally:
+        s.close()
