@@ -186,6 +186,19 @@ def peaks():
         return 6650.0, "fallback"
 
 
+def combine_ranks(world, dev, elapsed_ms, e2e_ms, jobs, e2e_jobs, nodes):
+    """Whole-job figures: the slowest rank's times (max) and every rank's work (sum). The
+    only collectives of the bench; the solves themselves exchange nothing."""
+    if world <= 1:
+        return elapsed_ms, e2e_ms, jobs, e2e_jobs, nodes
+    import torch
+    t = torch.tensor([elapsed_ms, e2e_ms or 0.0], dtype=torch.float64, device=dev)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    c = torch.tensor([jobs, e2e_jobs, nodes], dtype=torch.float64, device=dev)
+    torch.distributed.all_reduce(c)
+    return t[0].item(), (t[1].item() if e2e_ms else None), c[0].item(), c[1].item(), c[2].item()
+
+
 def golden_check(tables):
     """Results the GPU finished for the first deals of the set (rank 0's) against the
     reference's tables in the committed fixture (tests/golden/k13_24.npz)."""
@@ -264,15 +277,8 @@ def our_arm(a, rank, world, local_rank):
         barrier()
 
     nodes = sum(st["nodes"] for st in stats)
-    if world > 1:
-        t = torch.tensor([elapsed_ms, e2e_ms or 0.0], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        elapsed_ms, e2e_ms = t[0].item(), (t[1].item() if e2e_ms else None)
-        c = torch.tensor([jobs, e2e_jobs, nodes], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(c)
-        jobs_all, e2e_jobs_all, nodes_all = c[0].item(), c[1].item(), c[2].item()
-    else:
-        jobs_all, e2e_jobs_all, nodes_all = jobs, e2e_jobs, nodes
+    elapsed_ms, e2e_ms, jobs_all, e2e_jobs_all, nodes_all = combine_ranks(
+        world, dev, elapsed_ms, e2e_ms, jobs, e2e_jobs, nodes)
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
