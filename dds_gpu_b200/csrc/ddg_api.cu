@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -786,3 +787,5 @@ void ddg_make_deals(uint64_t seed, int64_t first, int64_t n, int k, uint64_t* ha
 }
 
 }  // extern "C"
+
+#include "ddg_static.cuh"

@@ -166,6 +166,22 @@ int ddg_stream_close(ddg_stream* st, int drain, ddg_stats* st_out);
  * NULL = binary search). For many deals use ddg_solve_batch. */
 int ddg_solve_strain(ddg_solver* s, const uint64_t* hands4, int strain, const int* ns4, int* out4);
 
+/* No counterpart in the reference. A solve that allocates nothing, for callers that may
+ * not call cudaMalloc/cudaFree: a process whose device memory is already reserved by
+ * another allocator (a framework's caching pool), a latency-critical loop that cannot take
+ * cudaFree's device-wide synchronisation, or code that must not fail for lack of memory at
+ * run time. Its working memory is a static device array reserved when libddg.so's module
+ * loads: 256 lanes with 2^9-bucket TTs, their stacks and counters (42.6 MB); no solver
+ * object is needed. d_hands (n*4 uint64, 16-byte aligned) and d_out20 (n*20) are the
+ * caller's device buffers, n <= 1,048,576 deals (larger n: DDG_E_ARG); one job per
+ * (deal, strain), binary search, tricks equal to ddg_solve_batch's. The call only enqueues
+ * two memsets and one launch on `stream` (a cudaStream_t, NULL = legacy default) and does
+ * not wait. The first call on each device looks up the array's address
+ * (cudaGetSymbolAddress) and must come before any stream capture on that device. Calls
+ * share the array: they must not overlap (serialise them on one stream or synchronise in
+ * between); overlapping calls race and their results are undefined. */
+int ddg_solve_static(const uint64_t* d_hands, int64_t n, uint8_t* d_out20, void* stream);
+
 /* Checks a deal (4 disjoint hands of equal size 1..13); DDG_OK or DDG_E_ARG. */
 int ddg_check_deal(const uint64_t* hands4);
 
