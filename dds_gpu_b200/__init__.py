@@ -13,7 +13,7 @@ import os
 
 import numpy as np
 
-__all__ = ["Solver", "Stream", "DDGError", "make_deals", "check_deal", "library_path", "load_library"]
+__all__ = ["Solver", "Stream", "Guide", "DDGError", "make_deals", "check_deal", "library_path", "load_library"]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "_lib", "libddg.so")
@@ -81,6 +81,7 @@ def load_library():
     lib.ddg_solve_batch.argtypes = [P, P, ctypes.c_int64, P, ctypes.POINTER(_Stats)]
     lib.ddg_solve_batch_seeded.argtypes = [P, P, ctypes.c_int64, P, P, ctypes.POINTER(_Stats)]
     lib.ddg_solve_device.argtypes = [P, P, ctypes.c_int64, P, P, P, P, ctypes.POINTER(_Stats)]
+    lib.ddg_solve_device_ex.argtypes = [P, P, ctypes.c_int64, P, P, P, P, P, P, ctypes.POINTER(_Stats)]
     lib.ddg_solve_begin.argtypes = [P, P, ctypes.c_int64, P, P, P]
     lib.ddg_solve_continue.argtypes = [P, ctypes.c_double, P, P, P, ctypes.POINTER(_Stats),
                                        ctypes.POINTER(ctypes.c_int)]
@@ -93,6 +94,14 @@ def load_library():
     lib.ddg_stream_capacity.argtypes = [P]
     lib.ddg_stream_capacity.restype = ctypes.c_int64
     lib.ddg_stream_close.argtypes = [P, ctypes.c_int, ctypes.POINTER(_Stats)]
+    lib.ddg_guide_param_count.restype = ctypes.c_int64
+    lib.ddg_guide_create.argtypes = [ctypes.c_int, ctypes.c_int, P, ctypes.POINTER(P)]
+    lib.ddg_guide_destroy.argtypes = [P]
+    lib.ddg_guide_destroy.restype = None
+    lib.ddg_guide_get_params.argtypes = [P, P]
+    lib.ddg_guide_set_params.argtypes = [P, P]
+    lib.ddg_guide_train_step.argtypes = [P, P, P, P, P, ctypes.c_int, ctypes.c_float, P, P]
+    lib.ddg_guide_predict.argtypes = [P, P, ctypes.c_int64, P, P]
     lib.ddg_check_deal.argtypes = [P]
     lib.ddg_make_deals.argtypes = [ctypes.c_uint64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int, P]
     lib.ddg_make_deals.restype = None
@@ -174,11 +183,13 @@ class Solver:
         self.last_stats = st.as_dict()
         return out
 
-    def solve_device(self, d_hands, n, d_out, d_seeds=0, d_job_nodes=0, stream=0):
-        """Device-pointer form (ddg_solve_device): integer addresses of device buffers."""
+    def solve_device(self, d_hands, n, d_out, d_seeds=0, d_job_nodes=0, stream=0, d_hints=0, d_best=0):
+        """Device-pointer form (ddg_solve_device / _ex): integer addresses of device buffers;
+        d_hints / d_best = the guide's root leads in and best leads out (n*20 int8)."""
         st = _Stats()
-        _check(self._lib.ddg_solve_device(self._h, P(d_hands), n, P(d_seeds or None), P(d_out),
-                                          P(d_job_nodes or None), P(stream or None), ctypes.byref(st)))
+        _check(self._lib.ddg_solve_device_ex(self._h, P(d_hands), n, P(d_seeds or None), P(d_hints or None),
+                                             P(d_out), P(d_best or None), P(d_job_nodes or None),
+                                             P(stream or None), ctypes.byref(st)))
         self.last_stats = st.as_dict()
         return self.last_stats
 
@@ -257,3 +268,58 @@ class Stream:
             self.close()
         except Exception:
             pass
+
+
+class Guide:
+    """The learned guide (ddg_guide_*): an MLP trained and run on the GPU by libddg's own
+    tensor-core kernels; predicts NS-trick seeds and root leads for the solver."""
+
+    def __init__(self, device=0, max_rows=4096, params=None):
+        self._lib = load_library()
+        self._h = P()
+        p = None
+        if params is not None:
+            p = np.ascontiguousarray(params, dtype=np.float32).reshape(-1)
+            if p.size != self.param_count():
+                raise DDGError(f"guide parameters: {p.size} values, {self.param_count()} expected")
+        _check(self._lib.ddg_guide_create(device, max_rows, p.ctypes.data if p is not None else None,
+                                          ctypes.byref(self._h)))
+        self.max_rows = max_rows
+
+    @staticmethod
+    def param_count():
+        return int(load_library().ddg_guide_param_count())
+
+    def close(self):
+        if self._h:
+            self._lib.ddg_guide_destroy(self._h)
+            self._h = P()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def params(self):
+        out = np.empty(self.param_count(), dtype=np.float32)
+        _check(self._lib.ddg_guide_get_params(self._h, out.ctypes.data))
+        return out
+
+    def set_params(self, params):
+        p = np.ascontiguousarray(params, dtype=np.float32).reshape(-1)
+        _check(self._lib.ddg_guide_set_params(self._h, p.ctypes.data))
+
+    def step(self, d_hands, d_tricks20, d_best20, rows, lr, want_grad=False):
+        """One training step on example indices `rows` (deal*20 + strain*4 + declarer);
+        returns (mean loss, trick-head hits, labelled rows, gradients or None)."""
+        r = np.ascontiguousarray(rows, dtype=np.int64)
+        stats = np.zeros(3, dtype=np.float32)
+        grad = np.empty(self.param_count(), dtype=np.float32) if want_grad else None
+        _check(self._lib.ddg_guide_train_step(self._h, P(d_hands), P(d_tricks20), P(d_best20), r.ctypes.data,
+                                              r.size, lr, stats.ctypes.data,
+                                              grad.ctypes.data if grad is not None else None))
+        return float(stats[0]), float(stats[1]), float(stats[2]), grad
+
+    def predict(self, d_hands, n, d_seed20=0, d_hint20=0):
+        _check(self._lib.ddg_guide_predict(self._h, P(d_hands), n, P(d_seed20 or None), P(d_hint20 or None)))

@@ -359,6 +359,12 @@ static int wait_launch(ddg_solver* s) {
 
 int ddg_solve_device(ddg_solver* s, const uint64_t* d_hands, int64_t n, const int8_t* d_seed20,
                      uint8_t* d_out20, uint64_t* d_job_nodes, void* stream_v, ddg_stats* st) {
+  return ddg_solve_device_ex(s, d_hands, n, d_seed20, nullptr, d_out20, nullptr, d_job_nodes, stream_v, st);
+}
+
+int ddg_solve_device_ex(ddg_solver* s, const uint64_t* d_hands, int64_t n, const int8_t* d_seed20,
+                        const int8_t* d_hint20, uint8_t* d_out20, int8_t* d_best20, uint64_t* d_job_nodes,
+                        void* stream_v, ddg_stats* st) {
   if (!s) return fail(DDG_E_ARG, "null solver");
   if (n < 0 || (n > 0 && (!d_hands || !d_out20))) return fail(DDG_E_ARG, "bad batch arguments");
   if (st) memset(st, 0, sizeof(*st));
@@ -369,8 +375,11 @@ int ddg_solve_device(ddg_solver* s, const uint64_t* d_hands, int64_t n, const in
   s->sliced = false;  // a plain solve ends any resumable one
   cudaStream_t stream = (cudaStream_t)stream_v;
   BatchArgs a = make_args(s, d_hands, n, d_seed20, d_out20, d_job_nodes);
+  a.hint20 = d_hint20;
+  a.best20 = d_best20;
   CUDA_TRY(cudaMemsetAsync(s->counters, 0, CNT_WORDS * 8, stream));
   CUDA_TRY(cudaMemsetAsync(d_out20, 0xFF, (size_t)n * 20, stream));
+  if (d_best20) CUDA_TRY(cudaMemsetAsync(d_best20, 0xFF, (size_t)n * 20, stream));
   *(volatile int*)s->h_stop = 0;
   if (s->tasks) CUDA_TRY(cudaMemsetAsync(s->tasks, 0, sizeof(TaskPool), stream));
   if (s->d_job_end_ns) CUDA_TRY(cudaMemsetAsync(s->d_job_end_ns, 0, (size_t)a.n_jobs * 8, stream));
@@ -789,3 +798,4 @@ void ddg_make_deals(uint64_t seed, int64_t first, int64_t n, int k, uint64_t* ha
 }  // extern "C"
 
 #include "ddg_static.cuh"
+#include "ddg_guide_api.cuh"

@@ -71,6 +71,8 @@ struct BatchArgs {
   unsigned long long* comp_tail;           // completion records written so far
   long long ring_mask;
   u64 idle_ns;                             // a block whose lanes found no deal this long ends
+  const int8_t* hint20;  // n * 20 root leads to try first (learned guide), -1 = none; or null
+  int8_t* best20;        // n * 20 best leads found (the cutting root card), -1 = none; or null
 };
 
 // One finished deal of a stream: its sequence number and table; `flag` = record index + 1,
@@ -224,6 +226,12 @@ struct DevEnv {
   }
   __device__ __forceinline__ long long out_row(const Lane& L) const {
     return a->ring ? (L.deal & a->ring_mask) : L.deal;
+  }
+  __device__ __forceinline__ int root_hint(const Lane& L) {
+    return a->hint20 ? (int)a->hint20[out_row(L) * 20 + L.strain * 4 + L.decl] : -1;
+  }
+  __device__ __forceinline__ void root_best(const Lane& L, int card) {
+    if (a->best20) a->best20[out_row(L) * 20 + L.strain * 4 + L.decl] = (int8_t)card;
   }
   __device__ __forceinline__ void answer(const Lane& L, int ns) {
     a->out20[out_row(L) * 20 + L.strain * 4 + L.decl] = (uint8_t)((L.decl & 1) == 0 ? ns : 13 - ns);

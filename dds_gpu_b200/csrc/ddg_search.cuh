@@ -533,6 +533,7 @@ struct Lane {
 
 // Sets up the search of declarer `decl`'s lead (leader = decl + 1) at `target`.
 DDG_HD void start_search(Lane& L) {
+  fr_set_best(L.f, -1);  // no root card yet (a root decided without moves keeps none)
   L.p.leader = (L.decl + 1) & 3;
   L.p.nplayed = 0;
   L.p.ns_won = 0;
@@ -635,6 +636,12 @@ DDG_CALL void node_done(Lane& L, Env& env) {
     L.stage = ST_RET;
     return;
   }
+  // A root search that went the leader's way names the lead that did it (the cutting
+  // card): after the last such search it is a best lead for the answer.
+  if (L.task < 0 && (L.v != 0) == ((L.p.leader & 1) == 0)) {
+    const int b = fr_best(L.f);
+    if (b >= 0) env.root_best(L, b);
+  }
   int ans = root_result(L);
   if (ans < 0) {
     start_search(L);
@@ -732,8 +739,18 @@ DDG_HD void step_enter(Lane& L, Env& env) {
 
 template <class Env>
 DDG_CALL void step_moves(Lane& L, Env& env) {
-  if (L.stage == ST_MOVES_LEAD) gen_moves_lead(L.p, frame_hint(L.f), L.top, L.f);
-  else gen_moves_follow(L.p, L.f);
+  if (L.stage == ST_MOVES_LEAD) {
+    int hint = frame_hint(L.f);
+    // At a job's root with no TT move yet, an outside hint (the learned guide's lead) takes
+    // the TT move's place in the ordering; the searches still decide every answer.
+    if (hint < 0 && L.sp == 0 && L.task < 0) {
+      const int h = env.root_hint(L);
+      if (h >= 0 && h < 64 && (hand_at(L.p.h, L.p.leader) >> h & 1)) hint = h;
+    }
+    gen_moves_lead(L.p, hint, L.top, L.f);
+  } else {
+    gen_moves_follow(L.p, L.f);
+  }
   L.stage = ST_NEXT;
 }
 

@@ -121,6 +121,17 @@ int ddg_solve_batch_seeded(ddg_solver* s, const uint64_t* hands, int64_t n, cons
 int ddg_solve_device(ddg_solver* s, const uint64_t* d_hands, int64_t n, const int8_t* d_seed20,
                      uint8_t* d_out20, uint64_t* d_job_nodes, void* stream, ddg_stats* st);
 
+/* ddg_solve_device with the learned guide's two seams (device buffers, n*20, indexed
+ * [deal][strain][declarer] like the results; NULL = unused): d_hint20 = a lead card
+ * (suit*16+rank) to try first at the job's root while the TT has no move for it (-1 =
+ * none; cards not in the leader's hand are ignored) - the reference's move-hint seam,
+ * src/dd.h:562,594-600; d_best20 receives a best lead for each answer (the root card that
+ * decided the last search going the leader's way, -1 when no lead was needed), the labels
+ * of the guide's move head (src/dd.h:847). Seeds, hints and labels never change a trick. */
+int ddg_solve_device_ex(ddg_solver* s, const uint64_t* d_hands, int64_t n, const int8_t* d_seed20,
+                        const int8_t* d_hint20, uint8_t* d_out20, int8_t* d_best20, uint64_t* d_job_nodes,
+                        void* stream, ddg_stats* st);
+
 /* Resumable (time-sliced) solve of n deals on device buffers. ddg_solve_begin sets it up
  * (results = 255 until solved); each ddg_solve_continue runs it for at most `seconds` and
  * returns with every lane's search state kept in device memory, so the next call goes on
@@ -165,6 +176,35 @@ int ddg_stream_close(ddg_stream* st, int drain, ddg_stats* st_out);
  * dd_solve_strain (src/dd.h:926) and dd_solve_strain_guess (src/dd.h:915; ns4 = NS seeds,
  * NULL = binary search). For many deals use ddg_solve_batch. */
 int ddg_solve_strain(ddg_solver* s, const uint64_t* hands4, int strain, const int* ns4, int* out4);
+
+/* The learned guide (no counterpart in the reference; it plugs into the reference's seams
+ * for an N seed, src/dd.h:898-924, and a move hint, src/dd.h:562,594-600). An MLP of
+ * 217 inputs (52 cards x 4 owners one-hot, 5 strains, 4 leaders) -> 256 GELU -> 256 GELU
+ * -> 14 NS-trick classes + 52 lead-card scores, BF16 weights with FP32 accumulation, run
+ * forward and backward by this library's tcgen05 tensor-core kernels. Parameters: a flat
+ * fp32 array of ddg_guide_param_count() values: W1[256][256] (inputs padded to 256),
+ * b1[256], W2[256][256], b2[256], W3[80][256] (outputs padded to 80), b3[80]. An example
+ * is (deal, strain, declarer) = index deal*20 + strain*4 + declarer, leader = declarer+1. */
+typedef struct ddg_guide ddg_guide;
+int64_t ddg_guide_param_count(void);
+/* max_rows: examples per training step / inference pass, a multiple of 128. params: the
+ * initial parameters (NULL = zeros). */
+int ddg_guide_create(int device, int max_rows, const float* params, ddg_guide** out);
+void ddg_guide_destroy(ddg_guide* g);
+int ddg_guide_get_params(ddg_guide* g, float* params);
+int ddg_guide_set_params(ddg_guide* g, const float* params);
+/* One step on the examples rows[0..n_rows) of the deals d_hands with labels d_tricks20
+ * (the solver's tables, 255 = no label) and d_best20 (best leads, -1 = none): softmax
+ * cross-entropy of both heads (the lead head over the leader's cards), gradients by
+ * backpropagation, then Adam with learning rate lr (lr <= 0: no update). stats3 (optional,
+ * host) = mean loss, trick-head hits, labelled rows; grad_host (optional) = the gradients
+ * in the parameter layout. */
+int ddg_guide_train_step(ddg_guide* g, const uint64_t* d_hands, const uint8_t* d_tricks20, const int8_t* d_best20,
+                         const int64_t* rows_host, int n_rows, float lr, float* stats3, float* grad_host);
+/* For n deals: d_seed20 = predicted NS tricks per [strain][declarer] (seeds for
+ * ddg_solve_batch_seeded / ddg_solve_device_ex) and d_hint20 = the leader's card with the
+ * highest lead score (for ddg_solve_device_ex); either may be NULL. Device buffers. */
+int ddg_guide_predict(ddg_guide* g, const uint64_t* d_hands, int64_t n, int8_t* d_seed20, int8_t* d_hint20);
 
 /* No counterpart in the reference. A solve that allocates nothing, for callers that may
  * not call cudaMalloc/cudaFree: a process whose device memory is already reserved by
