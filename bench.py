@@ -12,7 +12,9 @@ HBM between slices), so each step is one kernel launch timed with CUDA events.
 
 Rank 0 prints one JSON line. `value` = (deal, strain) jobs finished by all ranks in the K
 timed slices / 5 / max over ranks of the timed device time: the reference's own headline
-metric ("full-job deals/s": finished jobs / 5 per second while the set is being solved).
+metric ("full-job deals/s": finished jobs / 5 per second while the set is being solved),
+with the learned guide's seeds and root leads when its weights file is there (`plain` =
+the same measurement without the guide, run first on the same set).
 Only finished, exact jobs count; work in progress at the end of the timed slices does
 not. `e2e` = the same through the host API with, every step, the deals copied in from
 pinned host memory and all results copied out. `roofline` = TT bytes the search moved
@@ -54,6 +56,7 @@ def parse():
     p.add_argument("--schedule", type=int, default=0, help="0 block-phase kernel, 1 queue kernel")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-guide", action="store_true", help="plain solver only (no learned guide)")
     return p.parse_args()
 
 
@@ -214,6 +217,7 @@ def our_arm(a, rank, world, local_rank):
     import numpy as np
     import torch
     import dds_gpu_b200 as ddg
+    import dds_gpu_b200.guide as ddg_guide
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
@@ -232,36 +236,69 @@ def our_arm(a, rank, world, local_rank):
         if world > 1:
             torch.distributed.barrier()
 
-    solver.begin(dev_in.data_ptr(), n, dev_out.data_ptr(), stream=cs)
-    for s in range(a.warmup):  # warm-up slices (untimed)
-        flush.zero_()
-        solver.resume(a.slice_s, stream=cs)
-    torch.cuda.synchronize(dev)
+    def window(d_seed=0, d_hint=0):
+        """W warm-up and K timed slices of one resumable solve of the set."""
+        solver.begin(dev_in.data_ptr(), n, dev_out.data_ptr(), d_seeds=d_seed, d_hints=d_hint, stream=cs)
+        for s in range(a.warmup):  # warm-up slices (untimed)
+            flush.zero_()
+            solver.resume(a.slice_s, stream=cs)
+        torch.cuda.synchronize(dev)
+        sampler = ClockSampler(local_rank)
+        stats = []
+        barrier()
+        torch.cuda.synchronize(dev)
+        sampler.start()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for s in range(a.steps):
+            flush.zero_()
+            stats.append(solver.resume(a.slice_s, stream=cs)[1])
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        barrier()
+        return stats, e0.elapsed_time(e1), sampler.stop(), dev_out.cpu().numpy()
 
-    sampler = ClockSampler(local_rank)
-    stats = []
-    barrier()
-    torch.cuda.synchronize(dev)
-    sampler.start()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for s in range(a.steps):
-        flush.zero_()
-        stats.append(solver.resume(a.slice_s, stream=cs)[1])
-    e1.record(stream)
-    torch.cuda.synchronize(dev)
-    barrier()
-    clocks = sampler.stop()
-    elapsed_ms = e0.elapsed_time(e1)
-    tables = dev_out.cpu().numpy()
+    # The learned guide (when its trained weights are there): NS seeds and root leads for
+    # the whole set, computed on the GPU before the solve.
+    d_seed = d_hint = None
+    guide_info = None
+    params = None if a.no_guide else ddg_guide.load_weights()
+    if params is not None:
+        guide = ddg.Guide(device=local_rank, max_rows=8192, params=params)
+        d_seed = torch.empty(n * 20, dtype=torch.int8, device=dev)
+        d_hint = torch.empty(n * 20, dtype=torch.int8, device=dev)
+        torch.cuda.synchronize(dev)
+        g0 = time.perf_counter()
+        guide.predict(dev_in.data_ptr(), n, d_seed.data_ptr(), d_hint.data_ptr())
+        guide_ms = 1e3 * (time.perf_counter() - g0)
+        guide.close()
+        guide_info = {"predict_ms": guide_ms, "rows": n * 20}
+
+    plain_stats, plain_ms, plain_clocks, plain_tables = window()
+    plain_jobs = sum(st["jobs_done"] for st in plain_stats)
+    if d_seed is not None:
+        stats, elapsed_ms, clocks, tables = window(d_seed.data_ptr(), d_hint.data_ptr())
+        seeds = d_seed.cpu().numpy().reshape(n, 5, 4).astype(int)
+        t = tables.reshape(n, 5, 4).astype(int)
+        ns = np.where(np.arange(4) % 2 == 0, t, 13 - t)
+        done = t <= 13
+        guide_info.update({"seed_exact": float((seeds == ns)[done].mean()) if done.any() else None,
+                           "seed_within_one": float((abs(seeds - ns) <= 1)[done].mean()) if done.any() else None})
+    else:
+        stats, elapsed_ms, clocks, tables = plain_stats, plain_ms, plain_clocks, plain_tables
     jobs = sum(st["jobs_done"] for st in stats)
+    # equal tables where both runs finished: the guide changes the work, never an answer
+    both = (plain_tables != 255) & (tables != 255)
+    guided_equal_plain = bool((plain_tables[both] == tables[both]).all())
 
     # End to end through the host API: each step copies the deals in from pinned host memory,
     # runs the slice and copies every result out.
     e2e_ms, e2e_jobs = None, 0
     if not a.no_e2e:
         host_out = torch.empty((n, 20), dtype=torch.uint8).pin_memory()
-        solver.begin(dev_in.data_ptr(), n, dev_out.data_ptr(), stream=cs)
+        solver.begin(dev_in.data_ptr(), n, dev_out.data_ptr(), stream=cs,
+                     d_seeds=d_seed.data_ptr() if d_seed is not None else 0,
+                     d_hints=d_hint.data_ptr() if d_hint is not None else 0)
         for s in range(a.warmup):
             solver.resume(a.slice_s, hands_host=host_in.data_ptr(), out_host=host_out.data_ptr(), stream=cs)
         barrier()
@@ -279,6 +316,8 @@ def our_arm(a, rank, world, local_rank):
     nodes = sum(st["nodes"] for st in stats)
     elapsed_ms, e2e_ms, jobs_all, e2e_jobs_all, nodes_all = combine_ranks(
         world, dev, elapsed_ms, e2e_ms, jobs, e2e_jobs, nodes)
+    plain_ms_all, _, plain_jobs_all, _, plain_nodes_all = combine_ranks(
+        world, dev, plain_ms, None, plain_jobs, 0, sum(st["nodes"] for st in plain_stats))
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
@@ -310,9 +349,16 @@ def our_arm(a, rank, world, local_rank):
         "warmup": a.warmup, "ms_per_step": elapsed_ms / a.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
         "config": config_dict(a, world, {"lanes": stats[0]["lanes"] if stats else 0, "block": a.block,
-                                         "schedule": a.schedule, "guide": "off (plain DDS move order)"}),
+                                         "schedule": a.schedule,
+                                         "guide": ("learned guide: NS seeds (stepping search) + root leads"
+                                                   if guide_info else "off (plain DDS move order)")}),
         "jobs_finished": int(jobs_all), "nodes_per_s": nodes_all / (elapsed_ms * 1e-3),
         "nodes_per_finished_job": nodes_all / max(1, jobs_all),
+        "plain": {"value": plain_jobs_all / JPD / (plain_ms_all * 1e-3), "unit": "deals/s",
+                  "jobs_finished": int(plain_jobs_all),
+                  "nodes_per_finished_job": plain_nodes_all / max(1, plain_jobs_all)},
+        "guide": guide_info,
+        "guided_tables_equal_plain": guided_equal_plain,
         "golden_check": golden_check(tables),
         "warp_efficiency": eff,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -13,7 +13,7 @@ import os
 
 import numpy as np
 
-__all__ = ["Solver", "Stream", "Guide", "DDGError", "make_deals", "check_deal", "library_path", "load_library"]
+__all__ = ["Solver", "Stream", "Guide", "DDGError", "make_deals", "make_deals_mixed", "check_deal", "library_path", "load_library"]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "_lib", "libddg.so")
@@ -81,8 +81,10 @@ def load_library():
     lib.ddg_solve_batch.argtypes = [P, P, ctypes.c_int64, P, ctypes.POINTER(_Stats)]
     lib.ddg_solve_batch_seeded.argtypes = [P, P, ctypes.c_int64, P, P, ctypes.POINTER(_Stats)]
     lib.ddg_solve_device.argtypes = [P, P, ctypes.c_int64, P, P, P, P, ctypes.POINTER(_Stats)]
+    lib.ddg_solve_graph.argtypes = [P, P, ctypes.c_int64, P, P, P, ctypes.POINTER(_Stats)]
     lib.ddg_solve_device_ex.argtypes = [P, P, ctypes.c_int64, P, P, P, P, P, P, ctypes.POINTER(_Stats)]
     lib.ddg_solve_begin.argtypes = [P, P, ctypes.c_int64, P, P, P]
+    lib.ddg_solve_begin_ex.argtypes = [P, P, ctypes.c_int64, P, P, P, P]
     lib.ddg_solve_continue.argtypes = [P, ctypes.c_double, P, P, P, ctypes.POINTER(_Stats),
                                        ctypes.POINTER(ctypes.c_int)]
     lib.ddg_solve_strain.argtypes = [P, P, ctypes.c_int, P, P]
@@ -105,6 +107,9 @@ def load_library():
     lib.ddg_check_deal.argtypes = [P]
     lib.ddg_make_deals.argtypes = [ctypes.c_uint64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int, P]
     lib.ddg_make_deals.restype = None
+    lib.ddg_make_deals_mixed.argtypes = [ctypes.c_uint64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_double, P]
+    lib.ddg_make_deals_mixed.restype = None
     _lib = lib
     return lib
 
@@ -119,6 +124,15 @@ def make_deals(seed, first, n, k=13):
     out = np.zeros((n, 4), dtype=np.uint64)
     if n:
         load_library().ddg_make_deals(ctypes.c_uint64(seed), first, n, k, out.ctypes.data)
+    return out
+
+
+def make_deals_mixed(seed, first, n, k_min=5, k_max=13, skew=0.3):
+    """Uneven-hardness deals (ddg_make_deals_mixed): K ~ U{k_min..k_max}, a share `skew`
+    with a 7-10 card suit facing a void. (n, 4) uint64."""
+    out = np.zeros((n, 4), dtype=np.uint64)
+    if n:
+        load_library().ddg_make_deals_mixed(ctypes.c_uint64(seed), first, n, k_min, k_max, skew, out.ctypes.data)
     return out
 
 
@@ -193,9 +207,10 @@ class Solver:
         self.last_stats = st.as_dict()
         return self.last_stats
 
-    def begin(self, d_hands, n, d_out, d_seeds=0, stream=0):
-        """Starts a resumable solve on device buffers (ddg_solve_begin)."""
-        _check(self._lib.ddg_solve_begin(self._h, P(d_hands), n, P(d_seeds or None), P(d_out), P(stream or None)))
+    def begin(self, d_hands, n, d_out, d_seeds=0, stream=0, d_hints=0):
+        """Starts a resumable solve on device buffers (ddg_solve_begin_ex)."""
+        _check(self._lib.ddg_solve_begin_ex(self._h, P(d_hands), n, P(d_seeds or None), P(d_hints or None),
+                                            P(d_out), P(stream or None)))
 
     def resume(self, seconds, hands_host=0, out_host=0, stream=0):
         """Runs the resumable solve for at most `seconds` (ddg_solve_continue); returns
@@ -206,6 +221,14 @@ class Solver:
                                             P(stream or None), ctypes.byref(st), ctypes.byref(fin)))
         self.last_stats = st.as_dict()
         return bool(fin.value), self.last_stats
+
+    def solve_graph(self, d_hands, n, d_out, d_seeds=0, stream=0):
+        """The batch solve as a replayed CUDA graph (ddg_solve_graph)."""
+        st = _Stats()
+        _check(self._lib.ddg_solve_graph(self._h, P(d_hands), n, P(d_seeds or None), P(d_out), P(stream or None),
+                                         ctypes.byref(st)))
+        self.last_stats = st.as_dict()
+        return self.last_stats
 
     def set_job_times(self, d_job_end_ns):
         """Device buffer (integer address, n*jobs_per_deal uint64) for job completion times."""

@@ -67,6 +67,11 @@ struct ddg_solver {
   int64_t slice_n = 0;
   bool sliced = false, slice_done = false;
   bool streaming = false;  // a ddg_stream owns the lanes until it is closed
+  // CUDA graph of one batch solve (ddg_solve_graph): rebuilt when its arguments change.
+  cudaGraphExec_t graph = nullptr;
+  const void* graph_key[4] = {nullptr, nullptr, nullptr, nullptr};
+  int64_t graph_n = -1;
+  int graph_grid = 0;
 };
 
 extern "C" {
@@ -145,6 +150,7 @@ void ddg_solver_destroy(ddg_solver* s) {
   cudaFree(s->counters);
   cudaFree(s->tasks);
   cudaFree(s->save);
+  if (s->graph) cudaGraphExecDestroy(s->graph);
   cudaFree(s->d_hands);
   cudaFree(s->d_out);
   cudaFree(s->d_seeds);
@@ -394,8 +400,68 @@ int ddg_solve_device_ex(ddg_solver* s, const uint64_t* d_hands, int64_t n, const
   return read_stats(s, grid, st, c);
 }
 
+int ddg_solve_graph(ddg_solver* s, const uint64_t* d_hands, int64_t n, const int8_t* d_seed20, uint8_t* d_out20,
+                    void* stream_v, ddg_stats* st) {
+  if (!s) return fail(DDG_E_ARG, "null solver");
+  if (n <= 0 || !d_hands || !d_out20) return fail(DDG_E_ARG, "bad batch arguments");
+  if ((reinterpret_cast<uintptr_t>(d_hands) & 15) != 0) return fail(DDG_E_ARG, "hands not 16-byte aligned");
+  if (s->streaming) return fail(DDG_E_STATE, "a stream is open on this solver");
+  if (st) memset(st, 0, sizeof(*st));
+  CUDA_TRY(cudaSetDevice(s->device));
+  s->sliced = false;
+  cudaStream_t stream = (cudaStream_t)stream_v;
+  const bool same = s->graph && s->graph_n == n && s->graph_key[0] == d_hands && s->graph_key[1] == d_seed20 &&
+                    s->graph_key[2] == d_out20 && s->graph_key[3] == s->d_job_end_ns;
+  if (!same) {
+    if (s->graph) cudaGraphExecDestroy(s->graph);
+    s->graph = nullptr;
+    // The solve as one graph: clear the counters, the tables, the task pool, launch.
+    cudaStream_t cap = nullptr;
+    CUDA_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+    BatchArgs a = make_args(s, d_hands, n, d_seed20, d_out20, nullptr);
+    a.job_end_ns = s->d_job_end_ns;
+    cudaGraph_t g = nullptr;
+    int grid = 0, rc = DDG_OK;
+    cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->counters, 0, CNT_WORDS * 8, cap);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_out20, 0xFF, (size_t)n * 20, cap);
+    if (e == cudaSuccess && s->tasks) e = cudaMemsetAsync(s->tasks, 0, sizeof(TaskPool), cap);
+    if (e == cudaSuccess && s->d_job_end_ns) e = cudaMemsetAsync(s->d_job_end_ns, 0, (size_t)a.n_jobs * 8, cap);
+    if (e == cudaSuccess) rc = launch_batch(s, a, a.n_jobs, cap, &grid);
+    cudaError_t e2 = cudaStreamEndCapture(cap, &g);
+    if (e == cudaSuccess) e = e2;
+    if (e == cudaSuccess && rc == DDG_OK) e = cudaGraphInstantiate(&s->graph, g, 0);
+    if (g) cudaGraphDestroy(g);
+    cudaStreamDestroy(cap);
+    if (rc) return rc;
+    if (e != cudaSuccess) {
+      s->graph = nullptr;
+      return fail(DDG_E_CUDA, "solve graph: %s", cudaGetErrorString(e));
+    }
+    s->graph_n = n;
+    s->graph_key[0] = d_hands;
+    s->graph_key[1] = d_seed20;
+    s->graph_key[2] = d_out20;
+    s->graph_key[3] = s->d_job_end_ns;
+    s->graph_grid = grid;
+  }
+  *(volatile int*)s->h_stop = 0;
+  CUDA_TRY(cudaEventRecord(s->ev0, stream));
+  CUDA_TRY(cudaGraphLaunch(s->graph, stream));
+  CUDA_TRY(cudaEventRecord(s->ev1, stream));
+  int rc = wait_launch(s);
+  if (rc) return rc;
+  unsigned long long c[CNT_WORDS];
+  return read_stats(s, s->graph_grid, st, c);
+}
+
 int ddg_solve_begin(ddg_solver* s, const uint64_t* d_hands, int64_t n, const int8_t* d_seed20, uint8_t* d_out20,
                     void* stream_v) {
+  return ddg_solve_begin_ex(s, d_hands, n, d_seed20, nullptr, d_out20, stream_v);
+}
+
+int ddg_solve_begin_ex(ddg_solver* s, const uint64_t* d_hands, int64_t n, const int8_t* d_seed20,
+                       const int8_t* d_hint20, uint8_t* d_out20, void* stream_v) {
   if (!s) return fail(DDG_E_ARG, "null solver");
   if (n <= 0 || !d_hands || !d_out20) return fail(DDG_E_ARG, "bad batch arguments");
   if ((reinterpret_cast<uintptr_t>(d_hands) & 15) != 0) return fail(DDG_E_ARG, "hands not 16-byte aligned");
@@ -412,6 +478,7 @@ int ddg_solve_begin(ddg_solver* s, const uint64_t* d_hands, int64_t n, const int
   }
   cudaStream_t stream = (cudaStream_t)stream_v;
   s->slice_args = make_args(s, d_hands, n, d_seed20, d_out20, nullptr);
+  s->slice_args.hint20 = d_hint20;
   s->slice_args.save = s->save;
   s->slice_args.resume = 0;
   s->slice_n = n;
@@ -792,6 +859,68 @@ void ddg_make_deals(uint64_t seed, int64_t first, int64_t n, int k, uint64_t* ha
     uint64_t* h = hands + d * 4;
     h[0] = h[1] = h[2] = h[3] = 0;
     for (int i = 0; i < 4 * k; i++) h[i % 4] |= 1ull << cards[i];
+  }
+}
+
+void ddg_make_deals_mixed(uint64_t seed, int64_t first, int64_t n, int k_min, int k_max, double skew,
+                          uint64_t* hands) {
+  if (k_min < 1) k_min = 1;
+  if (k_max > 13) k_max = 13;
+  if (k_max < k_min) k_max = k_min;
+  for (int64_t d = 0; d < n; d++) {
+    uint64_t x = seed ^ (0x9E6C63D0676A9A99ull * (uint64_t)(first + d + 1));
+    const int k = k_min + (int)(splitmix_next(x) % (uint64_t)(k_max - k_min + 1));
+    uint64_t* h = hands + d * 4;
+    h[0] = h[1] = h[2] = h[3] = 0;
+    // A skewed deal: seat `lng` holds min(7..10, k) cards of suit `su`, seat `vd` none.
+    const bool skewed = (double)(splitmix_next(x) >> 11) * (1.0 / 9007199254740992.0) < skew;
+    int cards[52], m = 0;
+    for (int i = 0; i < 52; i++) cards[i] = (i / 13) * 16 + i % 13;
+    for (int i = 51; i > 0; i--) {  // shuffle all 52 first
+      int j = (int)(splitmix_next(x) % (uint64_t)(i + 1));
+      int t = cards[i];
+      cards[i] = cards[j];
+      cards[j] = t;
+    }
+    int cnt[4] = {0, 0, 0, 0};
+    int su = -1, lng = -1, vd = -1;
+    if (skewed) {
+      su = (int)(splitmix_next(x) % 4);
+      lng = (int)(splitmix_next(x) % 4);
+      vd = (lng + 1 + (int)(splitmix_next(x) % 3)) % 4;
+      int want = 7 + (int)(splitmix_next(x) % 4);
+      if (want > k) want = k;
+      for (int i = 0; i < 52 && cnt[lng] < want; i++)
+        if (cards[i] >= 0 && (cards[i] >> 4) == su) {
+          h[lng] |= 1ull << cards[i];
+          cnt[lng]++;
+          cards[i] = -1;
+        }
+    }
+    // The void seat first (only cards of the other suits), then the rest in shuffled order,
+    // round-robin over the seats that still need cards.
+    if (skewed)
+      for (int i = 0; i < 52 && cnt[vd] < k; i++)
+        if (cards[i] >= 0 && (cards[i] >> 4) != su) {
+          h[vd] |= 1ull << cards[i];
+          cnt[vd]++;
+          cards[i] = -1;
+        }
+    int seat = 0;
+    for (int i = 0; i < 52; i++) {
+      const int c = cards[i];
+      if (c < 0) continue;
+      for (int tries = 0; tries < 4; tries++, seat = (seat + 1) % 4) {
+        if (cnt[seat] >= k) continue;
+        if (seat == vd && (c >> 4) == su) continue;
+        h[seat] |= 1ull << c;
+        cnt[seat]++;
+        seat = (seat + 1) % 4;
+        break;
+      }
+      if (cnt[0] >= k && cnt[1] >= k && cnt[2] >= k && cnt[3] >= k) break;
+    }
+    (void)m;
   }
 }
 

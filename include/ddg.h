@@ -121,6 +121,14 @@ int ddg_solve_batch_seeded(ddg_solver* s, const uint64_t* hands, int64_t n, cons
 int ddg_solve_device(ddg_solver* s, const uint64_t* d_hands, int64_t n, const int8_t* d_seed20,
                      uint8_t* d_out20, uint64_t* d_job_nodes, void* stream, ddg_stats* st);
 
+/* ddg_solve_device as one CUDA graph (counter, table and task-pool clears and the
+ * persistent solve kernel), instantiated on the first call and replayed while d_hands,
+ * n, d_seed20 and d_out20 stay the same (a new set rebuilds it); the solver's job-time
+ * buffer, when set, is part of the graph. No counterpart in the reference (its batch is a
+ * plain launch, gpu/gpu_main.cu:256). */
+int ddg_solve_graph(ddg_solver* s, const uint64_t* d_hands, int64_t n, const int8_t* d_seed20, uint8_t* d_out20,
+                    void* stream, ddg_stats* st);
+
 /* ddg_solve_device with the learned guide's two seams (device buffers, n*20, indexed
  * [deal][strain][declarer] like the results; NULL = unused): d_hint20 = a lead card
  * (suit*16+rank) to try first at the job's root while the TT has no move for it (-1 =
@@ -145,6 +153,9 @@ int ddg_solve_begin(ddg_solver* s, const uint64_t* d_hands, int64_t n, const int
                     uint8_t* d_out20, void* stream);
 int ddg_solve_continue(ddg_solver* s, double seconds, const uint64_t* hands_host, uint8_t* out20_host,
                        void* stream, ddg_stats* st, int* finished);
+/* ddg_solve_begin with the guide's root leads (d_hint20, as in ddg_solve_device_ex). */
+int ddg_solve_begin_ex(ddg_solver* s, const uint64_t* d_hands, int64_t n, const int8_t* d_seed20,
+                       const int8_t* d_hint20, uint8_t* d_out20, void* stream);
 
 /* Streams (continuous batching; the reference's dd_stream, gpu/stream_main.cu:38-114,
  * 189-332). A stream keeps the solver's lanes running as one persistent kernel that takes
@@ -230,6 +241,13 @@ int ddg_check_deal(const uint64_t* hands4);
  * made alone. Cards 0..4k-1 of the shuffle go round-robin to N,E,S,W (as the reference's
  * random_deals, gpu/gpu_main.cu:154-163). hands: n*4. */
 void ddg_make_deals(uint64_t seed, int64_t first, int64_t n, int k, uint64_t* hands);
+
+/* Uneven-hardness deals: K drawn uniformly from k_min..k_max cards per seat, and a share
+ * `skew` of the deals skewed: one seat holds min(7..10, K) cards of one suit and another
+ * seat is void in it (the rest dealt round-robin from the shuffle). No counterpart in the
+ * reference (its configurations name the workload, not a generator). hands: n*4. */
+void ddg_make_deals_mixed(uint64_t seed, int64_t first, int64_t n, int k_min, int k_max, double skew,
+                          uint64_t* hands);
 
 #ifdef __cplusplus
 }

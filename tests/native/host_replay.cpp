@@ -37,6 +37,8 @@ struct HostEnv {
   void task_started() { start_nodes = st.nodes; }
   u64 tt_key_ = 0;
   u64& tt_key() { return tt_key_; }
+  int root_hint(const Lane&) { return -1; }
+  void root_best(const Lane&, int) {}
 
   bool take(Lane& L) {
     long long job = (*next)++;

@@ -104,3 +104,41 @@ def test_guide_trains_on_gpu_and_guided_solves_stay_exact(ddg):
     finally:
         guide.close()
         s.close()
+
+
+def test_trained_guide_saves_nodes(ddg):
+    """The committed guide against the plain solver on fresh deals: the same tables, and
+    fewer search nodes over the jobs both runs finished within the same time."""
+    import torch
+    import dds_gpu_b200.guide as ddg_guide
+    params = ddg_guide.load_weights()
+    if params is None:
+        pytest.skip("no trained guide weights")
+    n = 2000
+    hands = ddg.make_deals(12345, 0, n, 13)
+    d_h = to_dev(hands, np.int64)
+    guide = ddg.Guide(max_rows=4096, params=params)
+    d_seed = torch.empty(n * 20, dtype=torch.int8, device="cuda")
+    d_hint = torch.empty(n * 20, dtype=torch.int8, device="cuda")
+    guide.predict(d_h.data_ptr(), n, d_seed.data_ptr(), d_hint.data_ptr())
+    guide.close()
+    runs = []
+    for guided in (False, True):
+        s = ddg.Solver(tt_log2=10, jobs_per_deal=5, block=256, min_blocks=2, time_limit_s=12.0)
+        try:
+            d_out = torch.empty(n * 20, dtype=torch.uint8, device="cuda")
+            d_nodes = torch.zeros(n * 5, dtype=torch.int64, device="cuda")
+            s.solve_device(d_h.data_ptr(), n, d_out.data_ptr(), d_job_nodes=d_nodes.data_ptr(),
+                           d_seeds=d_seed.data_ptr() if guided else 0, d_hints=d_hint.data_ptr() if guided else 0)
+            runs.append((d_out.cpu().numpy().reshape(n, 5, 4), d_nodes.cpu().numpy()))
+        finally:
+            s.close()
+    (t0, n0), (t1, n1) = runs
+    both = (n0 > 0) & (n1 > 0)
+    assert both.sum() > 1000
+    fin = both.reshape(n, 5)
+    assert (t0[fin] == t1[fin]).all()
+    plain, guided = int(n0[both].sum()), int(n1[both].sum())
+    print(f"guide: {both.sum()} jobs finished by both, nodes plain {plain}, guided {guided} "
+          f"({guided / plain:.3f})")
+    assert guided < plain
