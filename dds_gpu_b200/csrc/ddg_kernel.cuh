@@ -71,6 +71,7 @@ struct BatchArgs {
   unsigned long long* comp_tail;           // completion records written so far
   long long ring_mask;
   u64 idle_ns;                             // a block whose lanes found no deal this long ends
+  int spread;            // phases hand their lanes round-robin over the block's warps
   const int8_t* hint20;  // n * 20 root leads to try first (learned guide), -1 = none; or null
   int8_t* best20;        // n * 20 best leads found (the cutting root card), -1 = none; or null
 };
@@ -329,12 +330,16 @@ __device__ __forceinline__ void run_phase(BlockShared<BLOCK>& sh, long long base
   const unsigned m = __ballot_sync(0xFFFFFFFFu, want);
   if (ln == 0) sh.mask[wid] = m;
   __syncthreads();
+  // Position of this thread in the phase's list: packed (thread t takes item t, so the
+  // items fill whole warps) or spread (item p goes to lane p / warps of warp p % warps, so
+  // every warp of the block takes a share and fewer lanes share each warp's divergence).
+  const int pos = sh.args.spread ? (tid & 31) * (BLOCK / 32) + wid : tid;
   int total = 0, item = -1;
 #pragma unroll
   for (int w = 0; w < BLOCK / 32; w++) {
     const unsigned mw = sh.mask[w];
     const int c = __popc(mw);
-    if (item < 0 && tid < total + c) item = w * 32 + select_bit(mw, tid - total);
+    if (item < 0 && pos < total + c) item = w * 32 + select_bit(mw, pos - total);
     total += c;
   }
   if (tid == 0 && total) {

@@ -56,6 +56,8 @@ typedef struct ddg_config {
   int free_below;       /* a block with fewer busy lanes than this runs each lane on its own
                            thread (no phases): faster lanes in the batch's tail. 0 = 64, -1 = never */
   int free_steps;       /* stages per lane per free-running round; 0 = 256 */
+  int phase_spread;     /* block-phase kernel: 0 = a phase's lanes fill whole warps in turn;
+                           1 = they go round-robin over all warps of the block */
 } ddg_config;
 
 /* Counters of one solve call (device-side counters, summed over lanes). */
