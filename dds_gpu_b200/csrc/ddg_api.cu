@@ -306,6 +306,7 @@ static BatchArgs make_args(ddg_solver* s, const uint64_t* d_hands, int64_t n, co
   a.free_steps = s->cfg.free_steps > 0 ? s->cfg.free_steps : 256;
   a.next_job = s->counters + CNT_NEXT_JOB;
   a.spread = s->cfg.phase_spread;
+  a.cheap_limit = s->cfg.cheap_limit == 0 ? 2 : s->cfg.cheap_limit < 0 ? 0 : s->cfg.cheap_limit;
   return a;
 }
 

@@ -72,6 +72,7 @@ struct BatchArgs {
   long long ring_mask;
   u64 idle_ns;                             // a block whose lanes found no deal this long ends
   int spread;            // phases hand their lanes round-robin over the block's warps
+  int cheap_limit;       // most cheap stages a lane runs per pass (0 = until it needs more)
   const int8_t* hint20;  // n * 20 root leads to try first (learned guide), -1 = none; or null
   int8_t* best20;        // n * 20 best leads found (the cutting root card), -1 = none; or null
 };
@@ -165,6 +166,7 @@ struct DevEnv {
   __device__ __forceinline__ u64 work_nodes() { return c->s.nodes - c->start_nodes; }
   __device__ __forceinline__ void task_started() { c->start_nodes = c->s.nodes; }
   __device__ __forceinline__ u64& tt_key() { return c->tt_key; }
+  __device__ __forceinline__ int cheap_limit() const { return a->cheap_limit; }
   // 1: a job; 0: no job will come; -1 (stream): none published yet.
   __device__ __forceinline__ int take(Lane& L) {
     unsigned long long job;

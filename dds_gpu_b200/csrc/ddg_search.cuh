@@ -984,7 +984,9 @@ DDG_HD bool cheap_stage(int st) {
 template <class Env>
 DDG_CALL void advance_cheap(Lane& L, Env& env) {
   bool offered = false;
-  for (;;) {
+  const int limit = env.cheap_limit();
+  for (int k = 1;; k++) {
+    if (limit && k > limit) return;  // the rest waits for the next pass
     switch (L.stage) {
       case ST_RET: step_ret(L, env); break;
       case ST_NEXT:

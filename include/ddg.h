@@ -58,6 +58,10 @@ typedef struct ddg_config {
   int free_steps;       /* stages per lane per free-running round; 0 = 256 */
   int phase_spread;     /* block-phase kernel: 0 = a phase's lanes fill whole warps in turn;
                            1 = they go round-robin over all warps of the block */
+  int cheap_limit;      /* most cheap stages (returns, next moves, job starts) a lane runs in
+                           one pass of the block-phase kernel: a lane with a long chain of
+                           returns no longer holds up the block's other phases; 0 = 2, -1 =
+                           no limit */
 } ddg_config;
 
 /* Counters of one solve call (device-side counters, summed over lanes). */

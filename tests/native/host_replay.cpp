@@ -38,6 +38,7 @@ struct HostEnv {
   u64 tt_key_ = 0;
   u64& tt_key() { return tt_key_; }
   int root_hint(const Lane&) { return -1; }
+  int cheap_limit() { return 0; }
   void root_best(const Lane&, int) {}
 
   bool take(Lane& L) {
