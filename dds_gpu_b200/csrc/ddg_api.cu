@@ -174,8 +174,8 @@ int ddg_solver_create(const ddg_config* cfg_in, ddg_solver** out) {
   }
   if (cfg.tt_log2 < TT_MIN_LOG2 || cfg.tt_log2 > 20)
     return fail(DDG_E_ARG, "tt_log2 %d is not in 9..20", cfg.tt_log2);
-  if (cfg.schedule != 0 && cfg.schedule != 1) return fail(DDG_E_ARG, "schedule %d is not 0 or 1", cfg.schedule);
-  const KVariant* variant = find_variant(cfg.block, cfg.min_blocks, cfg.schedule);
+  if (cfg.schedule < 0 || cfg.schedule > 2) return fail(DDG_E_ARG, "schedule %d is not 0, 1 or 2", cfg.schedule);
+  const KVariant* variant = find_variant(cfg.block, cfg.min_blocks, cfg.schedule == 1 ? 1 : 0);
   if (!variant)
     return fail(DDG_E_ARG, "no kernel for block %d / min_blocks %d (64/1, 128/1,4,6, 256/1..3)", cfg.block,
                 cfg.min_blocks);
@@ -306,7 +306,8 @@ static BatchArgs make_args(ddg_solver* s, const uint64_t* d_hands, int64_t n, co
   a.free_steps = s->cfg.free_steps > 0 ? s->cfg.free_steps : 256;
   a.next_job = s->counters + CNT_NEXT_JOB;
   a.spread = s->cfg.phase_spread;
-  a.cheap_limit = s->cfg.cheap_limit == 0 ? 2 : s->cfg.cheap_limit < 0 ? 0 : s->cfg.cheap_limit;
+  a.cheap_limit = s->cfg.cheap_limit == 0 ? 3 : s->cfg.cheap_limit < 0 ? 0 : s->cfg.cheap_limit;
+  a.fuse_follow = s->cfg.schedule == 2;
   return a;
 }
 
@@ -615,7 +616,7 @@ int ddg_stream_open(ddg_solver* s, int ring_slots, double idle_timeout_s, ddg_st
   *out = nullptr;
   if (!s) return fail(DDG_E_ARG, "null solver");
   if (s->streaming) return fail(DDG_E_STATE, "a stream is already open on this solver");
-  if (s->cfg.schedule != 0) return fail(DDG_E_ARG, "streams run on the block-phase kernel (schedule 0)");
+  if (s->cfg.schedule == 1) return fail(DDG_E_ARG, "streams run on the block-phase kernel (schedule 0 or 2)");
   if (ring_slots <= 0) ring_slots = 65536;
   if (ring_slots < 64 || ring_slots > (1 << 22) || (ring_slots & (ring_slots - 1)))
     return fail(DDG_E_ARG, "ring_slots %d is not a power of two in 64..4M", ring_slots);

@@ -73,6 +73,7 @@ struct BatchArgs {
   u64 idle_ns;                             // a block whose lanes found no deal this long ends
   int spread;            // phases hand their lanes round-robin over the block's warps
   int cheap_limit;       // most cheap stages a lane runs per pass (0 = until it needs more)
+  int fuse_follow;       // ENTER inside a trick runs in the cheap pass (no FOLLOW phase)
   const int8_t* hint20;  // n * 20 root leads to try first (learned guide), -1 = none; or null
   int8_t* best20;        // n * 20 best leads found (the cutting root card), -1 = none; or null
 };
@@ -167,6 +168,7 @@ struct DevEnv {
   __device__ __forceinline__ void task_started() { c->start_nodes = c->s.nodes; }
   __device__ __forceinline__ u64& tt_key() { return c->tt_key; }
   __device__ __forceinline__ int cheap_limit() const { return a->cheap_limit; }
+  __device__ __forceinline__ bool fuse_follow() const { return a->fuse_follow != 0; }
   // 1: a job; 0: no job will come; -1 (stream): none published yet.
   __device__ __forceinline__ int take(Lane& L) {
     unsigned long long job;

@@ -1001,6 +1001,10 @@ DDG_CALL void advance_cheap(Lane& L, Env& env) {
         step_take(L, env);
         if (L.stage == ST_TAKE) return;  // nothing to take yet
         break;
+      case ST_ENTER:  // inside a trick, ENTER is short: run it here when the schedule says so
+        if (L.p.nplayed == 0 || !env.fuse_follow()) return;
+        step_enter(L, env);
+        break;
       case ST_WAIT:
         if (!step_wait(L, env)) return;
         break;

@@ -45,7 +45,8 @@ typedef struct ddg_config {
   int schedule;         /* 0: block-phase kernel (all warps of a block run each stage phase
                            in turn over the block's compacted lanes); 1: queue kernel (each
                            warp takes up to 32 lanes from the fullest per-stage queue of its
-                           block, no block barriers) */
+                           block, no block barriers); 2: block-phase kernel with ENTER
+                           inside a trick run in the cheap pass (four phases, not five) */
   int min_blocks;       /* resident blocks per SM the kernel is compiled for (register cap):
                            block 64: 1; block 128: 1, 4, 6; block 256: 1..3; 0 = 1 */
   double time_limit_s;  /* stop after this many seconds (unfinished results = 255); 0 = none */
@@ -60,7 +61,7 @@ typedef struct ddg_config {
                            1 = they go round-robin over all warps of the block */
   int cheap_limit;      /* most cheap stages (returns, next moves, job starts) a lane runs in
                            one pass of the block-phase kernel: a lane with a long chain of
-                           returns no longer holds up the block's other phases; 0 = 2, -1 =
+                           returns no longer holds up the block's other phases; 0 = 3, -1 =
                            no limit */
 } ddg_config;
 
@@ -174,7 +175,7 @@ int ddg_solve_begin_ex(ddg_solver* s, const uint64_t* d_hands, int64_t n, const 
  * for nothing but a free lane: requests that arrive while others are on the GPU start as
  * lanes free up. Lanes that find no deal for idle_timeout_s (0 = 30 s) end; the next
  * submit or poll launches the kernel again. While a stream is open the solver's other
- * calls return DDG_E_STATE. Runs on the block-phase kernel (schedule 0), helping off. */
+ * calls return DDG_E_STATE. Runs on the block-phase kernel (schedule 0 or 2), helping off. */
 typedef struct ddg_stream ddg_stream;
 int ddg_stream_open(ddg_solver* s, int ring_slots, double idle_timeout_s, ddg_stream** out);
 int ddg_stream_submit(ddg_stream* st, const uint64_t* hands, int64_t n, int64_t* accepted);

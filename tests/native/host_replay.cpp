@@ -39,6 +39,7 @@ struct HostEnv {
   u64& tt_key() { return tt_key_; }
   int root_hint(const Lane&) { return -1; }
   int cheap_limit() { return 0; }
+  bool fuse_follow() { return false; }
   void root_best(const Lane&, int) {}
 
   bool take(Lane& L) {
