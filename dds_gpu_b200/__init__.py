@@ -145,7 +145,7 @@ def check_deal(hands4):
 class Solver:
     """A solver pool on one GPU (ddg_solver_create): per-lane TTs and stacks in HBM."""
 
-    def __init__(self, tt_log2=10, lanes=0, block=128, jobs_per_deal=5, device=0, schedule=0,
+    def __init__(self, tt_log2=10, lanes=0, block=256, jobs_per_deal=5, device=0, schedule=0,
                  time_limit_s=0.0, mem_fraction=0.85, min_blocks=0, help=0, free_below=0, free_steps=0,
                  phase_spread=0, cheap_limit=0):
         lib = load_library()

@@ -83,7 +83,8 @@ void ddg_config_default(ddg_config* c) {
   memset(c, 0, sizeof(*c));
   c->tt_log2 = 10;
   c->lanes = 0;
-  c->block = 128;
+  c->block = 256;
+  c->min_blocks = 2;
   c->jobs_per_deal = 5;
   c->device = 0;
   c->schedule = 0;
@@ -168,7 +169,8 @@ int ddg_solver_create(const ddg_config* cfg_in, ddg_solver** out) {
   if (cfg_in) {
     cfg = *cfg_in;
     if (!cfg.tt_log2) cfg.tt_log2 = 10;
-    if (!cfg.block) cfg.block = 128;
+    if (!cfg.block) cfg.block = 256;
+    if (!cfg.min_blocks) cfg.min_blocks = cfg.block == 256 ? 2 : 1;  // the measured best shape
     if (!cfg.jobs_per_deal) cfg.jobs_per_deal = 5;
     if (cfg.mem_fraction <= 0) cfg.mem_fraction = 0.85;
   }
