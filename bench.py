@@ -52,8 +52,8 @@ def parse():
     p.add_argument("--slice-s", type=float, default=4.0, help="seconds per step (one slice of the solve)")
     p.add_argument("--tt-log2", type=int, default=10)
     p.add_argument("--lanes", type=int, default=0, help="0 = fill the GPU")
-    p.add_argument("--block", type=int, default=256)
-    p.add_argument("--min-blocks", type=int, default=2)
+    p.add_argument("--block", type=int, default=0, help="threads (lanes) per block; 0 = library default (512)")
+    p.add_argument("--min-blocks", type=int, default=0)
     p.add_argument("--schedule", type=int, default=0, help="0 block-phase kernel, 1 queue kernel")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
@@ -344,7 +344,8 @@ def our_arm(a, rank, world, local_rank):
         "metric": METRIC, "value": value, "unit": "deals/s", "n_gpus": world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": elapsed_ms / a.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
-        "config": config_dict(a, world, {"lanes": stats[0]["lanes"] if stats else 0, "block": a.block,
+        "config": config_dict(a, world, {"lanes": stats[0]["lanes"] if stats else 0,
+                                         "block": stats[0]["block"] if stats else a.block,
                                          "schedule": a.schedule,
                                          "guide": ("learned guide: NS seeds (stepping search) + root leads"
                                                    if guide_info else "off (plain DDS move order)")}),
@@ -359,7 +360,7 @@ def our_arm(a, rank, world, local_rank):
         "warp_efficiency": eff,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                     "kernel": "ddg::batch_kernel<256,2>",
+                     "kernel": f"ddg::batch_kernel<{solver.block_shape}>",
                      "algorithmic_bytes": "TT bytes read+written per launch, counted in-kernel "
                                           f"({tt_bytes / max(1, nodes):.1f} B/node)"},
         "clocks": clocks,

@@ -145,7 +145,7 @@ def check_deal(hands4):
 class Solver:
     """A solver pool on one GPU (ddg_solver_create): per-lane TTs and stacks in HBM."""
 
-    def __init__(self, tt_log2=10, lanes=0, block=256, jobs_per_deal=5, device=0, schedule=0,
+    def __init__(self, tt_log2=10, lanes=0, block=0, jobs_per_deal=5, device=0, schedule=0,
                  time_limit_s=0.0, mem_fraction=0.85, min_blocks=0, help=0, free_below=0, free_steps=0,
                  phase_spread=0, cheap_limit=0):
         lib = load_library()
@@ -163,6 +163,8 @@ class Solver:
         self._h = P()
         _check(lib.ddg_solver_create(ctypes.byref(cfg), ctypes.byref(self._h)))
         self.config = {name: getattr(cfg, name) for name, _ in cfg._fields_}
+        blk = block or 512
+        self.block_shape = f"{blk}, {min_blocks or (2 if blk == 256 else 1)}"
         self.jobs_per_deal = jobs_per_deal
         self.last_stats = None
 

@@ -5,8 +5,9 @@
 Workload: (deal, strain) jobs over deals from ddg_make_deals_mixed (K uniform in 5..13
 cards per seat, 30 % skewed with a 7-10 card suit facing a void), seed 7.
 
-The tuner sweeps solver lanes, TT size (2^9..2^12 buckets per lane) and the kernel's stage
-schedule (block phases or per-warp queues); each candidate runs a short resumable slice
+The tuner sweeps the launch shape (512 threads x 1 block or 256 x 2 per SM), solver lanes,
+TT size (2^9..2^12 buckets per lane) and the kernel's stage schedule (block phases or
+per-warp queues); each candidate runs a short resumable slice
 of the same set and is scored by the jobs it finishes per second. The chosen setting
 then solves the whole set as one CUDA-graph launch of the persistent kernel (helping on,
 so idle lanes split the last hard jobs), with per-job completion times for the tail.
@@ -20,7 +21,8 @@ import numpy as np
 
 from . import DDGError, Solver, make_deals_mixed
 
-LANES = (16384, 32768, 49152, 0)  # 0 = every resident lane (148 SMs x 2 blocks x 256)
+LANES = (16384, 32768, 49152, 0)  # 0 = every resident lane (148 SMs x 512)
+SHAPES = ((512, 1), (256, 2))     # threads per block, resident blocks per SM
 TT_LOG2 = (9, 10, 11, 12)
 SCHEDULES = (0, 1)
 SEED = 7
@@ -28,8 +30,8 @@ SEED = 7
 
 def measure(cfg, d_hands, n, window_s, torch):
     """Jobs finished per second in one slice of `window_s` after a 1 s warm-up slice."""
-    s = Solver(tt_log2=cfg["tt_log2"], lanes=cfg["lanes"], block=256, min_blocks=2, jobs_per_deal=5,
-               schedule=cfg["schedule"])
+    s = Solver(tt_log2=cfg["tt_log2"], lanes=cfg["lanes"], block=cfg["block"], min_blocks=cfg["min_blocks"],
+               jobs_per_deal=5, schedule=cfg["schedule"])
     try:
         d_out = torch.empty(n * 20, dtype=torch.uint8, device=d_hands.device)
         s.begin(d_hands.data_ptr(), n, d_out.data_ptr())
@@ -42,8 +44,8 @@ def measure(cfg, d_hands, n, window_s, torch):
 
 def tune(d_hands, n, window_s, torch, log=print):
     results = []
-    for lanes, tt, sch in itertools.product(LANES, TT_LOG2, SCHEDULES):
-        cfg = {"lanes": lanes, "tt_log2": tt, "schedule": sch}
+    for (block, minb), lanes, tt, sch in itertools.product(SHAPES, LANES, TT_LOG2, SCHEDULES):
+        cfg = {"block": block, "min_blocks": minb, "lanes": lanes, "tt_log2": tt, "schedule": sch}
         try:
             rate, used = measure(cfg, d_hands, n, window_s, torch)
         except DDGError as e:  # e.g. the TTs do not fit
@@ -51,15 +53,15 @@ def tune(d_hands, n, window_s, torch, log=print):
             continue
         cfg["lanes"] = used
         results.append((rate, cfg))
-        log(f"  lanes {used:6d} TT 2^{tt} schedule {sch}: {rate:9.1f} jobs/s")
+        log(f"  block {block}x{minb} lanes {used:6d} TT 2^{tt} schedule {sch}: {rate:9.1f} jobs/s")
     results.sort(key=lambda r: -r[0])
     return results[0][1], results
 
 
 def run_batch(cfg, d_hands, n, limit_s, torch):
     """The whole set as one graph-launched persistent solve; completion-time tail."""
-    s = Solver(tt_log2=cfg["tt_log2"], lanes=cfg["lanes"], block=256, min_blocks=2, jobs_per_deal=5,
-               schedule=cfg["schedule"], help=1, time_limit_s=limit_s)
+    s = Solver(tt_log2=cfg["tt_log2"], lanes=cfg["lanes"], block=cfg["block"], min_blocks=cfg["min_blocks"],
+               jobs_per_deal=5, schedule=cfg["schedule"], help=1, time_limit_s=limit_s)
     try:
         d_out = torch.empty(n * 20, dtype=torch.uint8, device=d_hands.device)
         d_end = torch.zeros(n * 5, dtype=torch.int64, device=d_hands.device)
@@ -96,8 +98,8 @@ def main():
     d_hands = torch.from_numpy(hands.view(np.int64)).cuda()
     t0 = time.time()
     best, results = tune(d_hands, n, a.window, torch)
-    print(f"autotuner ({time.time() - t0:.0f} s): lanes {best['lanes']}, TT 2^{best['tt_log2']}, "
-          f"schedule {best['schedule']}", flush=True)
+    print(f"autotuner ({time.time() - t0:.0f} s): block {best['block']}x{best['min_blocks']}, lanes {best['lanes']}, "
+          f"TT 2^{best['tt_log2']}, schedule {best['schedule']}", flush=True)
     rep = run_batch(best, d_hands, n, a.limit, torch)
     rep.update({"workload": f"{n} deals from ddg_make_deals_mixed(seed {SEED}, K 5..13, 30% skewed), "
                             f"{a.jobs} (deal, strain) jobs, one CUDA-graph launch, helping on",

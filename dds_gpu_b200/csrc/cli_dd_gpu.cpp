@@ -77,7 +77,7 @@ int main(int argc, char** argv) {
   cfg.jobs_per_deal = env_int("PER_LEAD", 0) ? 20 : 5;
   cfg.device = env_int("DEVICE", 0);
   cfg.time_limit_s = getenv("TIME_LIMIT") ? atof(getenv("TIME_LIMIT")) : 0;
-  if (cfg.lanes > 0) cfg.lanes = (cfg.lanes + 255) / 256 * 256;  // whole blocks
+  if (cfg.lanes > 0) cfg.lanes = (cfg.lanes + cfg.block - 1) / cfg.block * cfg.block;  // whole blocks
   ddg_solver* s = nullptr;
   if (ddg_solver_create(&cfg, &s)) return die("solver");
   long jobs = n * cfg.jobs_per_deal;

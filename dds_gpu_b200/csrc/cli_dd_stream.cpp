@@ -67,11 +67,9 @@ int main(int argc, char** argv) {
   ddg_config_default(&cfg);
   cfg.tt_log2 = tt_log2;
   cfg.lanes = env_int("THREADS", 0);
-  cfg.block = 256;
-  cfg.min_blocks = 2;
   cfg.jobs_per_deal = env_int("PER_LEAD", 0) ? 20 : 5;
   cfg.device = env_int("DEVICE", 0);
-  if (cfg.lanes > 0) cfg.lanes = (cfg.lanes + 255) / 256 * 256;
+  if (cfg.lanes > 0) cfg.lanes = (cfg.lanes + cfg.block - 1) / cfg.block * cfg.block;
   ddg_solver* s = nullptr;
   if (ddg_solver_create(&cfg, &s)) return die("solver");
   ddg_stream* st = nullptr;

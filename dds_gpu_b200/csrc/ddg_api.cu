@@ -83,8 +83,8 @@ void ddg_config_default(ddg_config* c) {
   memset(c, 0, sizeof(*c));
   c->tt_log2 = 10;
   c->lanes = 0;
-  c->block = 256;
-  c->min_blocks = 2;
+  c->block = 512;
+  c->min_blocks = 1;
   c->jobs_per_deal = 5;
   c->device = 0;
   c->schedule = 0;
@@ -124,7 +124,7 @@ struct KVariant {
   }
 static const KVariant kVariants[] = {
     DDG_VARIANT(64, 1),  DDG_VARIANT(128, 1), DDG_VARIANT(128, 4), DDG_VARIANT(128, 6),
-    DDG_VARIANT(256, 1), DDG_VARIANT(256, 2), DDG_VARIANT(256, 3),
+    DDG_VARIANT(256, 1), DDG_VARIANT(256, 2), DDG_VARIANT(256, 3), DDG_VARIANT(512, 1),
 };
 #undef DDG_VARIANT
 
@@ -169,7 +169,7 @@ int ddg_solver_create(const ddg_config* cfg_in, ddg_solver** out) {
   if (cfg_in) {
     cfg = *cfg_in;
     if (!cfg.tt_log2) cfg.tt_log2 = 10;
-    if (!cfg.block) cfg.block = 256;
+    if (!cfg.block) cfg.block = 512;
     if (!cfg.min_blocks) cfg.min_blocks = cfg.block == 256 ? 2 : 1;  // the measured best shape
     if (!cfg.jobs_per_deal) cfg.jobs_per_deal = 5;
     if (cfg.mem_fraction <= 0) cfg.mem_fraction = 0.85;
@@ -179,7 +179,7 @@ int ddg_solver_create(const ddg_config* cfg_in, ddg_solver** out) {
   if (cfg.schedule < 0 || cfg.schedule > 2) return fail(DDG_E_ARG, "schedule %d is not 0, 1 or 2", cfg.schedule);
   const KVariant* variant = find_variant(cfg.block, cfg.min_blocks, cfg.schedule == 1 ? 1 : 0);
   if (!variant)
-    return fail(DDG_E_ARG, "no kernel for block %d / min_blocks %d (64/1, 128/1,4,6, 256/1..3)", cfg.block,
+    return fail(DDG_E_ARG, "no kernel for block %d / min_blocks %d (64/1, 128/1,4,6, 256/1..3, 512/1)", cfg.block,
                 cfg.min_blocks);
   if (cfg.jobs_per_deal != 5 && cfg.jobs_per_deal != 20)
     return fail(DDG_E_ARG, "jobs_per_deal %d is not 5 or 20", cfg.jobs_per_deal);

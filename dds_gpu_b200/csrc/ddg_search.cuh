@@ -461,6 +461,21 @@ DDG_HD int task_claim(TaskPool& tp, int start) {
   }
   return -1;
 }
+// Reads task k written by a lane of another SM, after its state showed it published (a
+// claimed task's position) or finished (its result): an acquire fence, then loads from
+// L2, since this SM's L1 may still hold the slot's earlier contents.
+static_assert(sizeof(Task) % 8 == 0, "task records are read as 8-byte words");
+DDG_HD void task_read(const TaskPool& tp, int k, Task& out) {
+#ifdef __CUDA_ARCH__
+  __threadfence();
+  const unsigned long long* s = reinterpret_cast<const unsigned long long*>(&tp.t[k]);
+  unsigned long long* d = reinterpret_cast<unsigned long long*>(&out);
+#pragma unroll
+  for (int i = 0; i < (int)(sizeof(Task) / 8); i++) d[i] = __ldcg(s + i);
+#else
+  out = tp.t[k];
+#endif
+}
 // Takes an unclaimed task back; true when it was still queued.
 DDG_HD bool task_retract(TaskPool& tp, int k) {
   if (atom_cas(&tp.state[k], TASK_QUEUED, TASK_FREE) == TASK_QUEUED) {
@@ -816,7 +831,8 @@ DDG_CALL void step_next(Lane& L, Env& env) {
       L.stage = ST_WAIT;
       return;
     }
-    const Task& k = tp.t[t];
+    Task k;
+    task_read(tp, t, k);
     if (k.v == (int)ns_side(fr_seat(f))) {  // the donated part cut off
       fr_set_result(f, k.v);
       f.acc = k.r;
@@ -824,6 +840,7 @@ DDG_CALL void step_next(Lane& L, Env& env) {
     } else {
       f.acc |= k.r;
     }
+    fence_block();  // the result is read before the slot can be posted again
     tp.state[t] = TASK_FREE;
     fr_clear_task(f);
     break;
@@ -878,7 +895,8 @@ DDG_CALL bool step_hungry(Lane& L, Env& env) {
   atom_add(&tp.hungry, -1);
   atom_add(&tp.busy, 1);
   env.task_started();
-  const Task& k = tp.t[t];
+  Task k;
+  task_read(tp, t, k);
   L.p = k.pos;
   L.f.acc = k.acc;
   L.f.tried = k.tried;

@@ -99,7 +99,7 @@ def main():
     a = p.parse_args()
     hands = make_deals(TRAIN_SEED, 0, a.deals, 13)
     d_hands = torch.from_numpy(hands.view(np.int64)).cuda()
-    solver = Solver(tt_log2=10, jobs_per_deal=5, block=256, min_blocks=2, time_limit_s=a.seconds)
+    solver = Solver(tt_log2=10, jobs_per_deal=5, time_limit_s=a.seconds)
     t0 = time.time()
     d_tricks, d_best, st = label(solver, d_hands, a.deals, torch)
     solver.close()

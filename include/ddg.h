@@ -39,7 +39,7 @@ typedef struct ddg_solver ddg_solver;
 typedef struct ddg_config {
   int tt_log2;          /* TT buckets per lane = 2^tt_log2, 9..20; default 10 (320 KB per lane) */
   int lanes;            /* solver lanes (GPU threads, one search each); default: fill the GPU */
-  int block;            /* threads per block (lanes per block): 64, 128 or 256; default 256 */
+  int block;            /* threads per block (lanes per block): 64, 128, 256 or 512; default 512 */
   int jobs_per_deal;    /* 5 = one job per strain, the 4 leads share a TT; 20 = one per lead */
   int device;           /* CUDA device ordinal */
   int schedule;         /* 0: block-phase kernel (all warps of a block run each stage phase
@@ -48,8 +48,8 @@ typedef struct ddg_config {
                            block, no block barriers); 2: block-phase kernel with ENTER
                            inside a trick run in the cheap pass (four phases, not five) */
   int min_blocks;       /* resident blocks per SM the kernel is compiled for (register cap):
-                           block 64: 1; block 128: 1, 4, 6; block 256: 1..3; 0 = 2 for
-                           block 256, else 1 */
+                           block 64: 1; block 128: 1, 4, 6; block 256: 1..3; block 512: 1;
+                           0 = 2 for block 256, else 1 */
   double time_limit_s;  /* stop after this many seconds (unfinished results = 255); 0 = none */
   double mem_fraction;  /* largest share of free device memory the pool may take; default 0.85 */
   int help;             /* 1: once the job queue is empty, idle lanes take over untried sibling

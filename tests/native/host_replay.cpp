@@ -73,6 +73,7 @@ struct SimShared {
   TaskPool pool;
   int budget = 0;  // donations allowed this iteration
   bool eager = false;
+  int cheap_limit = 0;  // most cheap stages per lane per pass, as the GPU kernel's
 };
 struct SimEnv : HostEnv {
   SimShared* sh;
@@ -86,6 +87,7 @@ struct SimEnv : HostEnv {
   }
   void unreserve() { sh->pool.queued--; }
   int claim_start() { return lane_id * 61; }
+  int cheap_limit() { return sh->cheap_limit; }
   u64 work_nodes() { return st.nodes - start_nodes + (u64)DONATE_MIN_NODES - (u64)min_nodes; }
 };
 
@@ -95,7 +97,7 @@ extern "C" {
 // lane could (not only when lanes are hungry). Results and nodes as replay_solve; stats[12]
 // = tasks posted, stats[13] = block iterations.
 int replay_block(const uint64_t* hands, long long n, int tt_log2, int jpd, int lanes, int eager, int free_below,
-                 int free_steps, int* out20, uint64_t* stats) {
+                 int free_steps, int* out20, uint64_t* stats, int cheap_limit) {
   if (tt_log2 < TT_MIN_LOG2 || tt_log2 > 16 || (jpd != 5 && jpd != 20) || lanes < 1 || lanes > 1024) return -1;
   std::atomic<long long> next{0};
   SimShared* sh = new SimShared();
@@ -127,6 +129,7 @@ int replay_block(const uint64_t* hands, long long n, int tt_log2, int jpd, int l
     L[i].task = -1;
   }
   sh->eager = eager != 0;
+  sh->cheap_limit = cheap_limit;
   uint64_t iters = 0;
   for (;;) {
     int live = 0;

@@ -12,13 +12,13 @@ from conftest import load_golden
 P = ctypes.c_void_p
 
 
-def block(lib, hands, lanes, eager, jpd=5, tt_log2=10, free_below=0, free_steps=64):
+def block(lib, hands, lanes, eager, jpd=5, tt_log2=10, free_below=0, free_steps=64, cheap_limit=0):
     n = hands.shape[0]
     h = np.ascontiguousarray(hands, dtype=np.uint64)
     out = np.zeros(n * 20, np.int32)
     st = np.zeros(14, np.uint64)
     rc = lib.replay_block(h.ctypes.data_as(P), ctypes.c_longlong(n), tt_log2, jpd, lanes, eager, free_below,
-                          free_steps, out.ctypes.data_as(P), st.ctypes.data_as(P))
+                          free_steps, out.ctypes.data_as(P), st.ctypes.data_as(P), cheap_limit)
     return rc, out.reshape(n, 5, 4), st
 
 
@@ -39,3 +39,15 @@ def test_helping_full_deals(replay_lib):
     idx = [1, 3, 15]
     rc, t, st = block(replay_lib, g["hands"][idx], 32, 1, 20)
     assert rc == 0 and (t == g["tricks"][idx]).all() and st[12] > 0
+
+
+@pytest.mark.parametrize("name", ["k6_120.npz", "k9_120.npz"])
+@pytest.mark.parametrize("cheap_limit", [1, 2, 3])
+@pytest.mark.parametrize("lanes,eager,jpd", [(16, 1, 20), (64, 1, 5), (32, 0, 20)])
+def test_helping_with_cheap_limit(replay_lib, name, cheap_limit, lanes, eager, jpd):
+    """The GPU kernel's cheap pass stops a lane after a few stages; helping must stay exact
+    when a lane is left mid-chain (in NEXT, RET, WAIT or HUNGRY) between passes."""
+    g = load_golden(name)
+    rc, t, st = block(replay_lib, g["hands"][:48], lanes, eager, jpd, cheap_limit=cheap_limit)
+    assert rc == 0
+    assert (t == g["tricks"][:48]).all()
