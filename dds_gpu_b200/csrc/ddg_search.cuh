@@ -21,7 +21,7 @@ namespace ddg {
 struct Pos {
   u64 h[4];
   u32 trick;  // cards of the current trick in play order, a byte each
-  int trump, leader, nplayed, ns_won, left;
+  int8_t trump, leader, nplayed, ns_won, left;  // small: lanes live in shared memory
 };
 
 // One level of the search (48 bytes; 16-byte aligned in the lane's stack).
