@@ -271,12 +271,15 @@ int64_t ddg_solver_bytes(const ddg_solver* s) { return s ? (int64_t)s->bytes : 0
 
 static int launch_batch(ddg_solver* s, const BatchArgs& a, long long n_jobs, cudaStream_t stream,
                         int* grid_out) {
-  // With helping every resident lane is launched: lanes without a job help the others.
-  long long want = (a.tasks || n_jobs > s->lanes) ? s->lanes : n_jobs;
-  int grid = (int)((want + s->block - 1) / s->block);
+  // Every lane is launched: the first jobs are dealt round-robin over the blocks, so a small
+  // batch spreads over all SMs (lanes without a job end at once, or help with helping on).
+  (void)n_jobs;
+  int grid = (int)((s->lanes + s->block - 1) / s->block);
   if (grid < 1) grid = 1;
   *grid_out = grid;
   BatchArgs args = a;
+  const long long lanes = (long long)grid * s->block;
+  args.rr_jobs = a.ring ? 0 : (a.n_jobs < lanes ? a.n_jobs : lanes);
   void* params[] = {&args};
   CUDA_TRY(cudaLaunchKernel((const void*)s->variant->fn, dim3(grid), dim3(s->block), params, s->variant->smem,
                             stream));

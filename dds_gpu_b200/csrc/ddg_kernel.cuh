@@ -73,6 +73,7 @@ struct BatchArgs {
   u64 idle_ns;                             // a block whose lanes found no deal this long ends
   int spread;            // phases hand their lanes round-robin over the block's warps
   int cheap_limit;       // most cheap stages a lane runs per pass (0 = until it needs more)
+  long long rr_jobs;     // jobs 0..rr_jobs-1 are dealt to the lanes round-robin over the blocks
   int fuse_follow;       // ENTER inside a trick runs in the cheap pass (no FOLLOW phase)
   const int8_t* hint20;  // n * 20 root leads to try first (learned guide), -1 = none; or null
   int8_t* best20;        // n * 20 best leads found (the cutting root card), -1 = none; or null
@@ -119,6 +120,7 @@ __device__ __forceinline__ void lane_begin(const BatchArgs& a, long long lane, L
     return;
   }
   L.stage = ST_TAKE;
+  L.job = -1;  // no job yet in this launch
   L.sp = 0;
   L.gen = a.lane_gen[lane];
   L.v = 0;
@@ -179,7 +181,13 @@ struct DevEnv {
       L.deal = L.job / a->jpd;
       hands = a->ring + (L.deal & a->ring_mask) * 4;
     } else {
-      job = atomicAdd(a->next_job, 1ull);
+      // A lane's first job of the launch is dealt round-robin over the blocks (job j to
+      // block j mod grid), so a batch with fewer jobs than lanes spreads over every SM
+      // instead of filling the first blocks; later jobs come from the shared counter.
+      const long long t = lane - (long long)blockIdx.x * blockDim.x;
+      const long long rr = t * gridDim.x + blockIdx.x;
+      if (L.job < 0 && rr < a->rr_jobs) job = (unsigned long long)rr;
+      else job = atomicAdd(a->next_job, 1ull) + (unsigned long long)a->rr_jobs;
       if ((long long)job >= a->n_jobs) return 0;
       L.job = (long long)job;
       L.deal = L.job / a->jpd;
