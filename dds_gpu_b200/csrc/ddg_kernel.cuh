@@ -153,6 +153,7 @@ struct DevEnv {
   LaneCounters* c;
   TaskPool* tp;           // null when helping is off
   const int* help_hint;   // block flag: hungry lanes outnumber queued tasks (this iteration)
+  int* take_budget;       // stream: deals this block may still start this iteration
   long long lane;
 
   __device__ __forceinline__ LaneStats& stats() { return c->s; }
@@ -176,7 +177,12 @@ struct DevEnv {
     unsigned long long job;
     const u64* hands;
     if (a->ring) {
-      if (!stream_take(job)) return *reinterpret_cast<const volatile int*>(a->closing) && !stream_more() ? 0 : -1;
+      // A block takes its share of the waiting jobs per iteration, so that a few deals in
+      // flight spread over all SMs instead of filling the block that polled first.
+      const bool closing = *reinterpret_cast<const volatile int*>(a->closing) != 0;
+      if (closing && !stream_more()) return 0;  // nothing more will come
+      if (atomicSub(take_budget, 1) <= 0) return -1;
+      if (!stream_take(job)) return -1;
       L.job = (long long)job;
       L.deal = L.job / a->jpd;
       hands = a->ring + (L.deal & a->ring_mask) * 4;
@@ -283,6 +289,7 @@ struct BlockShared {
   unsigned long long ph_warps[PH_COUNT], ph_items[PH_COUNT], iters;
   int stop;
   int help_hint;    // hungry lanes outnumber queued tasks (read once per iteration)
+  int take_budget;  // stream: jobs this block may still take this iteration
   int claim_slots;  // hungry lanes of this block that may look for a task this iteration
   int all_done;     // no job left anywhere and no lane busy: hungry lanes stop
   unsigned long long ph_cycles[PH_COUNT];
@@ -322,6 +329,7 @@ __device__ __forceinline__ DevEnv lane_env(BlockShared<BLOCK>& sh, long long lan
   env.c = &sh.cnt[slot];
   env.tp = sh.args.tasks;
   env.help_hint = &sh.help_hint;
+  env.take_budget = &sh.take_budget;
   env.lane = lane;
   return env;
 }
@@ -426,6 +434,12 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(BatchArgs a) {
     }
     if (tid == 0) {
       sh.iters++;
+      if (a.ring) {  // this block's share of the jobs waiting in the ring
+        const long long waiting =
+            (long long)*reinterpret_cast<const volatile unsigned long long*>(a.published) * a.jpd -
+            (long long)*reinterpret_cast<const volatile unsigned long long*>(a.next_job);
+        sh.take_budget = (int)((waiting > 0 ? waiting : 0) / gridDim.x) + 1;
+      }
       if (a.tasks) {  // one read of the helping counters per block and iteration
         const int q = atom_load(&a.tasks->queued), h = atom_load(&a.tasks->hungry);
         sh.help_hint = h > q;
