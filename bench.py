@@ -38,7 +38,7 @@ sys.path.insert(0, ROOT)
 METRIC = "exact DD deals/s on 1 B200, learned-guided vs plain; nodes/deal; p99 ms"
 SET_SEED, SET_SIZE, SET_K = 2, 20000, 13
 JPD = 5
-DRAM_BYTES_PER_NODE = 53.4  # dram__bytes_read.sum + dram__bytes_write.sum per node, 13-card slice
+DRAM_BYTES_PER_NODE = 53.9  # dram__bytes_read.sum + dram__bytes_write.sum per node, 13-card slice
 WORKLOAD = ("13-card seeded random deals (20,000 per GPU), all 5 strains x 4 declarers, "
             "exact TT 2^10 buckets per lane, one job per (deal, strain)")
 
@@ -337,8 +337,8 @@ def our_arm(a, rank, world, local_rank):
     eff = {name: (ln[k] / (32.0 * it[k]) if it[k] else None)
            for k, name in enumerate(["cheap", "enter_lead", "enter_follow", "moves_lead", "moves_follow"])}
     # DRAM bytes per launch: the per-node DRAM traffic of one ncu capture of this kernel on a
-    # smaller case of the same workload (profiles/batch_kernel_13card_traffic.md), scaled
-    # by the nodes a bench launch searches.
+    # smaller case of the same workload (profiles/batch_kernel_13card_full.md), scaled by
+    # the nodes a bench launch searches.
     traffic = DRAM_BYTES_PER_NODE * nodes / max(1, len(stats))
     line = {
         "metric": METRIC, "value": value, "unit": "deals/s", "n_gpus": world, "steps": a.steps,
