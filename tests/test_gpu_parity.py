@@ -241,3 +241,20 @@ def test_stream_continuous_batching(ddg):
         assert (s.solve(hands[:4]) == want[:4]).all()
     finally:
         s.close()
+
+
+@pytest.mark.parametrize("block,min_blocks,schedule,cheap_limit,spread",
+                         [(512, 1, 0, 0, 0), (256, 2, 0, 0, 0), (512, 1, 2, 0, 0), (512, 1, 0, -1, 0),
+                          (512, 1, 0, 1, 0), (256, 2, 0, 0, 1), (128, 4, 0, 0, 0)])
+def test_launch_shapes_and_schedules(ddg, block, min_blocks, schedule, cheap_limit, spread):
+    """Every launch shape and stage schedule the autotuner may pick searches exactly the
+    reference's nodes, job for job."""
+    g = load_golden("k8_120.npz")
+    s = ddg.Solver(tt_log2=10, jobs_per_deal=5, lanes=4096, block=block, min_blocks=min_blocks,
+                   schedule=schedule, cheap_limit=cheap_limit, phase_spread=spread)
+    try:
+        t, nodes, st = device_solve(ddg, s, g["hands"])
+        assert (t == g["tricks"]).all()
+        assert (nodes == g["nodes_jpd5"]).all()
+    finally:
+        s.close()
