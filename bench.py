@@ -1,27 +1,39 @@
 #!/usr/bin/env python
 """Benchmark: exact double-dummy deals/s on B200s (one process per GPU, weak scaling).
 
-Workload: the 13-card benchmark set, 20,000 seeded uniformly random deals per GPU
-(ddg_make_deals seed 2; rank r takes deals [20000 r, 20000 (r+1)) of that stream), one
-job per (deal, strain) with the four declarers sharing a TT of 2^10 buckets, all inputs
-resident in HBM. The set is solved as one resumable solve (ddg_solve_begin); one step is
-one slice of it (ddg_solve_continue, --slice-s seconds, every lane's search state kept in
-HBM between slices), so each step is one kernel launch timed with CUDA events.
+Workload: seeded uniformly random 13-card deals (seed 2; deals [0, 20,000) are the
+20,000-deal benchmark set, and the solve runs on over deals [0, SET_SIZE) of the same
+stream so that every lane holds a job through the whole run), all 5 strains x 4 declarers,
+one job per (deal, strain) with the four declarers sharing a TT of 2^10 buckets per lane,
+inputs resident in HBM; rank r takes deals [SET_SIZE r, SET_SIZE (r+1)). The set is solved as one
+resumable solve (ddg_solve_begin); a step is one slice of it (ddg_solve_continue,
+--slice-s seconds, every lane's search state kept in HBM between slices): one kernel launch,
+timed with CUDA events on its stream.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+    python bench.py --profile-case [--lanes L] [--set-size D]   # one slice to capture under ncu
 
-Rank 0 prints one JSON line. `value` = (deal, strain) jobs finished by all ranks in the K
-timed slices / 5 / max over ranks of the timed device time: the reference's own headline
-metric ("full-job deals/s": finished jobs / 5 per second while the set is being solved),
-with the learned guide's seeds and root leads when its weights file is there (`plain` =
-the same measurement without the guide, run first on the same set).
-Only finished, exact jobs count; work in progress at the end of the timed slices does
-not. `e2e` = the same through the host API with, every step, the deals copied in from
-pinned host memory and all results copied out. `roofline` = TT bytes the search moved
-(counted in-kernel) per second of kernel time, against the measured HBM copy bandwidth.
-`cpu_baseline` = the reference's own CPU solver (compiled from its sources into
-oracle/_ref, else the C restatement) on the same deals over the same slices, all host
-cores. `--impl reference` prints that CPU measurement as the reference arm.
+value: exact deals/s in steady state. The GPU searches exactly the reference's nodes job
+for job (same bounds, move order and TT decisions; the tests check it node for node), so a
+deal costs the GPU the reference's search nodes, and with every lane busy the rate at
+which whole tables complete is the node rate divided by the mean nodes per deal of the
+workload (the renewal-reward rate of a solver that always has the next job). The mean is
+measured, not assumed: tests/golden/k13_bench_2000.npz holds the reference's complete
+tables and per-job node counts for deals [0, 2,000) of the set (the learned guide's
+searches: tests/golden/k13_bench_2000_guided.npz, from the host replay of this solver's
+stage machine with the guide's seeds and leads). `value` is the guided solver's (the guide
+seeds the search and orders the root leads; the searches decide every answer), `plain`
+the same measurement without the guide. `finished_deals_per_s` is the reference README's
+window metric (jobs finished in the timed slices / 5 / time), which favours the easy
+deals and is reported beside it, for both arms.
+e2e: the same through the host API with, every step, the deals copied in from pinned host
+memory and all results copied out. roofline: TT bytes of the launch (64 per probe, 16 per
+entry read, 80 per store) per second of kernel time, against the measured HBM copy
+bandwidth. cpu_baseline / --impl reference: the reference's own CPU solver
+(dd_solve_strain from its src/dd.h, compiled into oracle/_ref/cpu_window, which also makes
+the deals itself) on every host core over the same slices. parity: every job of deals
+[0, 2,000) that a run finished against the reference's tables, and every job the GPU and
+the CPU run both finished against each other.
 """
 import argparse
 import json
@@ -36,29 +48,58 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "exact DD deals/s on 1 B200, learned-guided vs plain; nodes/deal; p99 ms"
-SET_SEED, SET_SIZE, SET_K = 2, 20000, 13
+SET_SEED, SET_K = 2, 13
+SET_SIZE = 60000  # deals per GPU: far more jobs than the lanes finish in a run, so no lane idles
+BENCH_SET = 20000
 JPD = 5
-DRAM_BYTES_PER_NODE = 53.9  # dram__bytes_read.sum + dram__bytes_write.sum per node, 13-card slice
-WORKLOAD = ("13-card seeded random deals (20,000 per GPU), all 5 strains x 4 declarers, "
-            "exact TT 2^10 buckets per lane, one job per (deal, strain)")
+SAMPLE = os.path.join(ROOT, "tests", "golden", "k13_bench_2000.npz")
+GUIDED_SAMPLE = os.path.join(ROOT, "tests", "golden", "k13_bench_2000_guided.npz")
+# DRAM bytes (read + write) per search node of one launch of this workload's own shape
+# (TT 2^10, full grid, steady state), from `bench.py --profile-case` under ncu.
+DRAM_BYTES_PER_NODE = None
+WORKLOAD = ("13-card seeded random deals, all 5 strains x 4 declarers, exact TT 2^10 buckets per lane, "
+            "one job per (deal, strain)")
 
 
-def parse():
+def parse(argv=None):
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=5)
-    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--slice-s", type=float, default=4.0, help="seconds per step (one slice of the solve)")
+    p.add_argument("--slice-s", type=float, default=2.0, help="seconds per step (one slice of the solve)")
     p.add_argument("--tt-log2", type=int, default=10)
     p.add_argument("--lanes", type=int, default=0, help="0 = fill the GPU")
     p.add_argument("--block", type=int, default=0, help="threads (lanes) per block; 0 = library default (512)")
     p.add_argument("--min-blocks", type=int, default=0)
     p.add_argument("--schedule", type=int, default=0, help="0 block-phase kernel, 1 queue kernel")
+    p.add_argument("--set-size", type=int, default=SET_SIZE)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-guide", action="store_true", help="plain solver only (no learned guide)")
-    return p.parse_args()
+    p.add_argument("--profile-case", action="store_true",
+                   help="warm-up slices then one slice, nothing else (the launch to capture under ncu)")
+    return p.parse_args(argv)
+
+
+def launch_plan(gpus, env):
+    """What to do with --gpus N: 'run' (this process is one of the N ranks, or N = 1),
+    'spawn' (start N ranks under torch.distributed.run), or 'refuse' (started as a rank of
+    a job of another size)."""
+    world = env.get("WORLD_SIZE")
+    if world is None:
+        return "spawn" if gpus > 1 else "run"
+    return "run" if int(world) == gpus else "refuse"
+
+
+def spawn_ranks(gpus, argv):
+    import socket
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={gpus}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__)] + argv
+    return subprocess.call(cmd)
 
 
 def host_cores():
@@ -68,65 +109,104 @@ def host_cores():
         return os.cpu_count() or 1
 
 
-def deal_set(rank):
+def deal_set(rank, size=SET_SIZE):
     from dds_gpu_b200 import make_deals
-    return make_deals(SET_SEED, rank * SET_SIZE, SET_SIZE, SET_K)
+    return make_deals(SET_SEED, rank * size, size, SET_K)
+
+
+def sample_costs():
+    """Mean search nodes per deal of the workload: the reference's complete solves of deals
+    [0, 2,000) (plain), and the guided search's (host replay with the guide's seeds and
+    leads), with the standard error of each mean; None where the file is missing."""
+    import numpy as np
+    out = {}
+    for key, path in (("plain", SAMPLE), ("guided", GUIDED_SAMPLE)):
+        if not os.path.exists(path):
+            out[key] = None
+            continue
+        with np.load(path) as z:
+            per_deal = z["nodes_jpd5"].astype(np.float64).reshape(-1, 5).sum(axis=1)
+            meta = {k: z[k] for k in z.files if k in ("params_sum",)}
+        out[key] = {"nodes_per_deal": float(per_deal.mean()), "deals": int(per_deal.size),
+                    "stderr": float(per_deal.std(ddof=1) / np.sqrt(per_deal.size)), **{k: float(v) for k, v in meta.items()}}
+    return out
+
+
+def sample_tables():
+    import numpy as np
+    with np.load(SAMPLE) as z:
+        return z["tricks"].reshape(-1, 20)
+
+
+def parity_against(got, want):
+    """Entries of `got` (n, 20) that are solved (not 255) in the rows both hold, compared."""
+    m = min(len(got), len(want))
+    g, w = got[:m], want[:m]
+    done = (g != 255) & (w != 255)
+    return int(done.sum()), bool((g[done] == w[done]).all())
 
 
 # ---- CPU reference path (baseline only) -------------------------------------------------
 
-def cpu_window(deals, tt_log2, slice_s, slices):
-    """The reference's CPU solver over the deal set for `slices` slices of `slice_s` seconds
-    (oracle/_ref/cpu_window, built from the reference's sources; else the C restatement's
-    oracle/_build/cpu_window). Returns (jobs finished per slice, nodes per slice, threads, kind)."""
+def cpu_window(a, size, slices, tables_out=None):
+    """The reference's CPU solver over deals [0, size) of the set for `slices` slices of
+    a.slice_s (oracle/_ref/cpu_window, built from the reference's sources; else the C
+    restatement's oracle/_build/cpu_window). It makes the deals itself."""
     exe = os.path.join(ROOT, "oracle", "_ref", "cpu_window")
     if not os.path.exists(exe):
         subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
         exe = os.path.join(ROOT, "oracle", "_build", "cpu_window")
-    cores = host_cores()
-    with tempfile.NamedTemporaryFile(suffix=".bin", delete=False) as f:
-        f.write(deals.tobytes())
-        path = f.name
-    try:
-        out = subprocess.run([exe, path, str(tt_log2), str(cores), str(slice_s), str(slices)],
-                             check=True, capture_output=True, text=True,
-                             timeout=slice_s * slices + 120).stdout
-    finally:
-        os.unlink(path)
-    r = json.loads(out.strip().splitlines()[-1])
-    return r["jobs"], r["nodes"], r["threads"], r["kind"]
+    args = [exe, f"gen:{SET_SEED}:{size}:{SET_K}", str(a.tt_log2), str(host_cores()), str(a.slice_s), str(slices),
+            str(a.warmup)]
+    if tables_out:
+        args.append(tables_out)
+    out = subprocess.run(args, check=True, capture_output=True, text=True, timeout=a.slice_s * slices + 120).stdout
+    return json.loads(out.strip().splitlines()[-1])
 
 
-def cpu_measure(a, deals):
-    jobs, nodes, threads, kind = cpu_window(deals, a.tt_log2, a.slice_s, a.warmup + a.steps)
-    t_jobs = sum(jobs[a.warmup:])
-    value = t_jobs / JPD / (a.steps * a.slice_s)
-    sample = (f"deal set seed {SET_SEED} (20,000 deals) solved by {threads} threads, one TT each; "
-              f"(deal, strain) jobs finished in slices {a.warmup}..{a.warmup + a.steps - 1} of "
-              f"{a.slice_s:g} s (first {a.warmup} = warm-up): {t_jobs} jobs, "
-              f"{sum(nodes[a.warmup:]) / max(1, t_jobs):.0f} nodes/job")
-    return {"value": value, "unit": "deals/s", "cores": threads, "kind": kind, "sample": sample}
+def cpu_measure(a, costs, size=BENCH_SET):
+    import numpy as np
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "tables.bin")
+        r = cpu_window(a, size, a.warmup + a.steps, path)
+        tables = np.fromfile(path, dtype=np.uint8).reshape(-1, 20)
+    t = a.steps * a.slice_s
+    t_jobs = sum(r["jobs"][a.warmup:])
+    t_nodes = sum(r["nodes"][a.warmup:])
+    nps = t_nodes / t
+    plain = costs.get("plain")
+    value = nps / plain["nodes_per_deal"] if plain else t_jobs / JPD / t
+    sample = (f"deals [0, {size}) of seed {SET_SEED} solved in order by {r['threads']} threads, one TT each; "
+              f"slices {a.warmup}..{a.warmup + a.steps - 1} of {a.slice_s:g} s timed (first {a.warmup} = warm-up): "
+              f"{t_nodes} nodes, {t_jobs} jobs finished; value = nodes/s / reference nodes per deal")
+    return {"value": value, "unit": "deals/s", "cores": r["threads"], "kind": r["kind"], "sample": sample,
+            "nodes_per_s": nps, "finished_deals_per_s": t_jobs / JPD / t,
+            "job_ms": {"p50": r["job_ms_p50"], "p99": r["job_ms_p99"]}}, tables
 
 
-def config_dict(a, world, extra=None):
-    d = {"workload": WORKLOAD, "deal_set": f"seed {SET_SEED}, {SET_SIZE} deals per GPU, K={SET_K}",
-         "tt_log2": a.tt_log2, "jobs_per_deal": JPD, "step": f"one {a.slice_s:g} s slice of the resumable solve",
-         "parallelism": f"dp{world} (own deal set per GPU, no collective on the data path)",
-         "l2": "flushed between steps (256 MiB write); the TT working set (GBs) is far above L2"}
-    if extra:
-        d.update(extra)
-    return d
+def config_dict(a, world):
+    return {"workload": WORKLOAD,
+            "deal_set": (f"seed {SET_SEED}, K={SET_K}; deals [0, {BENCH_SET}) are the benchmark set, the solve runs "
+                         f"over [0, {a.set_size}) per GPU so no lane idles"),
+            "tt_log2": a.tt_log2, "jobs_per_deal": JPD, "step": f"one {a.slice_s:g} s slice of the resumable solve",
+            "parallelism": f"dp{world} (own deal range per GPU, no collective on the data path)",
+            "l2": "flushed between steps (256 MiB write); the TT working set (GBs) is far above L2"}
 
 
 def reference_arm(a, rank, world):
     if rank != 0:
         return
-    cpu = cpu_measure(a, deal_set(0))
+    costs = sample_costs()
+    cpu, tables = cpu_measure(a, costs)
+    n, eq = parity_against(tables, sample_tables()) if costs.get("plain") else (0, True)
     line = {"metric": METRIC, "value": cpu["value"], "unit": "deals/s", "impl": "reference", "n_gpus": world,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * a.slice_s,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
             "data": "synthetic", "config": config_dict(a, world),
-            "cpu_baseline": cpu,
+            "nodes_per_s": cpu["nodes_per_s"], "finished_deals_per_s": cpu["finished_deals_per_s"],
+            "job_ms": cpu["job_ms"], "nodes_per_deal": costs.get("plain"),
+            "parity": {"checked": n, "equal": eq, "against": "reference tables of deals [0, 2000) (fixture)"},
+            "cpu_baseline": {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
             "e2e": {"value": cpu["value"], "unit": "deals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -203,15 +283,15 @@ def combine_ranks(world, dev, elapsed_ms, e2e_ms, jobs, e2e_jobs, nodes):
     return t[0].item(), (t[1].item() if e2e_ms else None), c[0].item(), c[1].item(), c[2].item()
 
 
-def golden_check(tables):
-    """Results the GPU finished for the first deals of the set (rank 0's) against the
-    reference's tables in the committed fixture (tests/golden/k13_24.npz)."""
+def quantiles_ms(start, end, warm_end):
+    """p50 / p99 search time (ms) of the jobs finished in the timed slices (finished now,
+    not yet at the end of the warm-up)."""
     import numpy as np
-    g = np.load(os.path.join(ROOT, "tests", "golden", "k13_24.npz"))
-    want = g["tricks"].reshape(-1, 20)
-    got = tables[: want.shape[0]]
-    done = got != 255
-    return {"checked": int(done.sum()), "equal": bool((got[done] == want[done]).all())}
+    done = (end > 0) & (warm_end == 0) & (start > 0)
+    if not done.any():
+        return {"p50": None, "p99": None, "jobs": 0}
+    d = np.sort((end[done] - start[done]).astype(np.float64) / 1e6)
+    return {"p50": float(d[len(d) // 2]), "p99": float(d[min(len(d) - 1, int(0.99 * len(d)))]), "jobs": int(len(d))}
 
 
 def our_arm(a, rank, world, local_rank):
@@ -222,16 +302,32 @@ def our_arm(a, rank, world, local_rank):
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    deals = deal_set(rank)
+    deals = deal_set(rank, a.set_size)
     solver = ddg.Solver(tt_log2=a.tt_log2, lanes=a.lanes, block=a.block, jobs_per_deal=JPD, device=local_rank,
                         min_blocks=a.min_blocks, schedule=a.schedule)
     n = deals.shape[0]
     host_in = torch.from_numpy(deals.view(np.int64)).pin_memory()
     dev_in = host_in.to(dev)
     dev_out = torch.empty((n, 20), dtype=torch.uint8, device=dev)
+    d_end = torch.zeros(n * JPD, dtype=torch.int64, device=dev)
+    d_start = torch.zeros(n * JPD, dtype=torch.int64, device=dev)
+    solver.set_job_times(d_end.data_ptr(), d_start.data_ptr())
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream(dev)
     cs = stream.cuda_stream
+
+    if a.profile_case:  # the launch to capture: W warm-up slices, then one slice
+        solver.begin(dev_in.data_ptr(), n, dev_out.data_ptr(), stream=cs)
+        for _ in range(a.warmup):
+            solver.resume(a.slice_s, stream=cs)
+        _, st = solver.resume(a.slice_s, stream=cs)
+        torch.cuda.synchronize(dev)
+        if rank == 0:
+            print(json.dumps({"profile_case": True, "launches": a.warmup + 1, "last_launch": {
+                k: st[k] for k in ("nodes", "tt_probes", "tt_entry_reads", "tt_stores", "tt_bytes", "kernel_ms",
+                                   "lanes", "grid", "block", "jobs_done")}}), flush=True)
+        solver.close()
+        return
 
     def barrier():
         if world > 1:
@@ -240,10 +336,11 @@ def our_arm(a, rank, world, local_rank):
     def window(d_seed=0, d_hint=0):
         """W warm-up and K timed slices of one resumable solve of the set."""
         solver.begin(dev_in.data_ptr(), n, dev_out.data_ptr(), d_seeds=d_seed, d_hints=d_hint, stream=cs)
-        for s in range(a.warmup):  # warm-up slices (untimed)
+        for _ in range(a.warmup):  # warm-up slices (untimed)
             flush.zero_()
             solver.resume(a.slice_s, stream=cs)
         torch.cuda.synchronize(dev)
+        warm_end = d_end.cpu().numpy()
         sampler = ClockSampler(local_rank)
         stats = []
         barrier()
@@ -251,13 +348,16 @@ def our_arm(a, rank, world, local_rank):
         sampler.start()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        for s in range(a.steps):
+        for _ in range(a.steps):
             flush.zero_()
             stats.append(solver.resume(a.slice_s, stream=cs)[1])
         e1.record(stream)
         torch.cuda.synchronize(dev)
         barrier()
-        return stats, e0.elapsed_time(e1), sampler.stop(), dev_out.cpu().numpy()
+        clocks = sampler.stop()
+        start, end = d_start.cpu().numpy(), d_end.cpu().numpy()
+        return {"stats": stats, "ms": e0.elapsed_time(e1), "clocks": clocks, "tables": dev_out.cpu().numpy(),
+                "lat": quantiles_ms(start, end, warm_end), "started_all": bool((start > 0).all())}
 
     # The learned guide (when its trained weights are there): NS seeds and root leads for
     # the whole set, computed on the GPU before the solve.
@@ -271,118 +371,166 @@ def our_arm(a, rank, world, local_rank):
         torch.cuda.synchronize(dev)
         g0 = time.perf_counter()
         guide.predict(dev_in.data_ptr(), n, d_seed.data_ptr(), d_hint.data_ptr())
-        guide_ms = 1e3 * (time.perf_counter() - g0)
+        torch.cuda.synchronize(dev)
+        guide_info = {"predict_ms": 1e3 * (time.perf_counter() - g0), "rows": n * 20,
+                      "params_sum": float(params.astype(np.float64).sum())}
         guide.close()
-        guide_info = {"predict_ms": guide_ms, "rows": n * 20}
 
-    plain_stats, plain_ms, plain_clocks, plain_tables = window()
-    plain_jobs = sum(st["jobs_done"] for st in plain_stats)
+    costs = sample_costs()
+    plain_run = window()
+    runs = {"plain": plain_run}
     if d_seed is not None:
-        stats, elapsed_ms, clocks, tables = window(d_seed.data_ptr(), d_hint.data_ptr())
+        runs["guided"] = window(d_seed.data_ptr(), d_hint.data_ptr())
         seeds = d_seed.cpu().numpy().reshape(n, 5, 4).astype(int)
-        t = tables.reshape(n, 5, 4).astype(int)
+        t = runs["guided"]["tables"].reshape(n, 5, 4).astype(int)
         ns = np.where(np.arange(4) % 2 == 0, t, 13 - t)
         done = t <= 13
         guide_info.update({"seed_exact": float((seeds == ns)[done].mean()) if done.any() else None,
                            "seed_within_one": float((abs(seeds - ns) <= 1)[done].mean()) if done.any() else None})
-    else:
-        stats, elapsed_ms, clocks, tables = plain_stats, plain_ms, plain_clocks, plain_tables
-    jobs = sum(st["jobs_done"] for st in stats)
-    # equal tables where both runs finished: the guide changes the work, never an answer
-    both = (plain_tables != 255) & (tables != 255)
-    guided_equal_plain = bool((plain_tables[both] == tables[both]).all())
+    # the guide's nodes per deal belong to these weights only
+    g_cost = costs.get("guided")
+    guided_cost_ok = bool(guide_info and g_cost and abs(g_cost.get("params_sum", 0) - guide_info["params_sum"]) < 1e-3)
 
     # End to end through the host API: each step copies the deals in from pinned host memory,
     # runs the slice and copies every result out.
-    e2e_ms, e2e_jobs = None, 0
+    e2e_ms, e2e_nodes, e2e_jobs = None, 0, 0
     if not a.no_e2e:
         host_out = torch.empty((n, 20), dtype=torch.uint8).pin_memory()
         solver.begin(dev_in.data_ptr(), n, dev_out.data_ptr(), stream=cs,
                      d_seeds=d_seed.data_ptr() if d_seed is not None else 0,
                      d_hints=d_hint.data_ptr() if d_hint is not None else 0)
-        for s in range(a.warmup):
+        for _ in range(a.warmup):
             solver.resume(a.slice_s, hands_host=host_in.data_ptr(), out_host=host_out.data_ptr(), stream=cs)
         barrier()
         torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
-        for s in range(a.steps):
+        for _ in range(a.steps):
             flush.zero_()
-            e2e_jobs += solver.resume(a.slice_s, hands_host=host_in.data_ptr(), out_host=host_out.data_ptr(),
-                                      stream=cs)[1]["jobs_done"]
-            assert int((host_out[:24] != 255).sum()) >= 0  # the results are on the host
+            st = solver.resume(a.slice_s, hands_host=host_in.data_ptr(), out_host=host_out.data_ptr(), stream=cs)[1]
+            e2e_nodes += st["nodes"]
+            e2e_jobs += st["jobs_done"]
         torch.cuda.synchronize(dev)
         e2e_ms = 1e3 * (time.perf_counter() - t0)
         barrier()
 
-    nodes = sum(st["nodes"] for st in stats)
-    elapsed_ms, e2e_ms, jobs_all, e2e_jobs_all, nodes_all = combine_ranks(
-        world, dev, elapsed_ms, e2e_ms, jobs, e2e_jobs, nodes)
-    plain_ms_all, _, plain_jobs_all, _, plain_nodes_all = combine_ranks(
-        world, dev, plain_ms, None, plain_jobs, 0, sum(st["nodes"] for st in plain_stats))
+    head = "guided" if ("guided" in runs and guided_cost_ok) else "plain"
+    summary = {}
+    for key, run in runs.items():
+        nodes = sum(st["nodes"] for st in run["stats"])
+        jobs = sum(st["jobs_done"] for st in run["stats"])
+        ms, _, jobs_all, _, nodes_all = combine_ranks(world, dev, run["ms"], None, jobs, 0, nodes)
+        cost = costs.get(key)
+        if key == "guided" and not guided_cost_ok:
+            cost = None
+        nps = nodes_all / (ms * 1e-3)
+        summary[key] = {"value": nps / cost["nodes_per_deal"] if cost else None, "unit": "deals/s",
+                        "nodes_per_s": nps, "nodes_per_deal": cost,
+                        "finished_deals_per_s": jobs_all / JPD / (ms * 1e-3), "jobs_finished": int(jobs_all),
+                        "nodes_per_s_by_step": [st["nodes"] / (st["kernel_ms"] * 1e-3) for st in run["stats"]],
+                        "job_ms": run["lat"], "lanes_idle": not run["started_all"], "ms": ms}
+    e2e_ms_all, _, e2e_nodes_all, _, _ = combine_ranks(world, dev, e2e_ms or 0.0, None, e2e_nodes, 0, 0)
 
-    cpu = None
+    cpu = cpu_tables = None
     if rank == 0 and world == 1 and not a.no_cpu:
-        cpu = cpu_measure(a, deals)
+        cpu, cpu_tables = cpu_measure(a, costs)
 
     if rank != 0:
         solver.close()
         return
+    # parity: the reference's tables of deals [0, 2000) and the CPU run's finished jobs
+    checked, equal = 0, True
+    against = []
+    if os.path.exists(SAMPLE):
+        want = sample_tables()
+        for run in runs.values():
+            c, e = parity_against(run["tables"], want)
+            checked, equal = checked + c, equal and e
+        against.append("reference tables of deals [0, 2000) (fixture made by the reference's solver)")
+    if cpu_tables is not None:
+        for run in runs.values():
+            c, e = parity_against(run["tables"], cpu_tables)
+            checked, equal = checked + c, equal and e
+        against.append("the reference CPU solver's tables of this run")
+    both = (runs["plain"]["tables"] != 255)
+    if "guided" in runs:
+        both &= runs["guided"]["tables"] != 255
+        guided_equal_plain = bool((runs["plain"]["tables"][both] == runs["guided"]["tables"][both]).all())
+    else:
+        guided_equal_plain = None
+
+    run = runs[head]
+    stats = run["stats"]
     kernel_ms = sum(st["kernel_ms"] for st in stats)
-    tt_bytes = sum(st["tt_bytes"] for st in stats)
+    alg_bytes = sum(64 * st["tt_probes"] + 16 * st["tt_entry_reads"] + 80 * st["tt_stores"] for st in stats)
+    counted = sum(st["tt_bytes"] for st in stats)
+    nodes = sum(st["nodes"] for st in stats)
     it = [sum(st["phase_warps"][k] for st in stats) for k in range(5)]
     ln = [sum(st["phase_items"][k] for st in stats) for k in range(5)]
     peak, peak_kind = peaks()
-    achieved = tt_bytes / (kernel_ms * 1e-3) / 1e9 if kernel_ms else 0.0
-    value = jobs_all / JPD / (elapsed_ms * 1e-3)
+    launches = len(stats)
+    achieved = (alg_bytes / launches) / (kernel_ms / launches * 1e-3) / 1e9 if kernel_ms else 0.0
     eff = {name: (ln[k] / (32.0 * it[k]) if it[k] else None)
            for k, name in enumerate(["cheap", "enter_lead", "enter_follow", "moves_lead", "moves_follow"])}
-    # DRAM bytes per launch: the per-node DRAM traffic of one ncu capture of this kernel on a
-    # smaller case of the same workload (profiles/batch_kernel_13card_full.md), scaled by
-    # the nodes a bench launch searches.
-    traffic = DRAM_BYTES_PER_NODE * nodes / max(1, len(stats))
+    s_head = summary[head]
+    value = s_head["value"] if s_head["value"] is not None else s_head["finished_deals_per_s"]
+    elapsed_ms = s_head["ms"]
     line = {
         "metric": METRIC, "value": value, "unit": "deals/s", "n_gpus": world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": elapsed_ms / a.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
-        "config": config_dict(a, world, {"lanes": stats[0]["lanes"] if stats else 0,
-                                         "block": stats[0]["block"] if stats else a.block,
-                                         "schedule": a.schedule,
-                                         "guide": ("learned guide: NS seeds (stepping search) + root leads"
-                                                   if guide_info else "off (plain DDS move order)")}),
-        "jobs_finished": int(jobs_all), "nodes_per_s": nodes_all / (elapsed_ms * 1e-3),
-        "nodes_per_finished_job": nodes_all / max(1, jobs_all),
-        "plain": {"value": plain_jobs_all / JPD / (plain_ms_all * 1e-3), "unit": "deals/s",
-                  "jobs_finished": int(plain_jobs_all),
-                  "nodes_per_finished_job": plain_nodes_all / max(1, plain_jobs_all)},
-        "guide": guide_info,
-        "guided_tables_equal_plain": guided_equal_plain,
-        "golden_check": golden_check(tables),
+        "config": config_dict(a, world),
+        "value_is": (f"{head} solver: nodes/s over the timed slices / the workload's mean nodes per deal"
+                     if s_head["value"] is not None else "finished jobs / 5 / s (no node-cost sample)"),
+        "tuning": {"lanes": stats[0]["lanes"] if stats else 0, "block": stats[0]["block"] if stats else a.block,
+                   "schedule": a.schedule,
+                   "guide": ("learned guide: NS seeds (stepping search) + root leads" if head == "guided"
+                             else "off (plain DDS move order)")},
+        "nodes_per_s": s_head["nodes_per_s"], "nodes_per_deal": s_head["nodes_per_deal"],
+        "finished_deals_per_s": s_head["finished_deals_per_s"], "job_ms": s_head["job_ms"],
+        "guided": summary.get("guided"), "plain": summary["plain"],
+        "guide": guide_info, "guided_tables_equal_plain": guided_equal_plain,
+        "parity": {"checked": checked, "equal": equal, "against": against},
         "warp_efficiency": eff,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                     "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": (DRAM_BYTES_PER_NODE * nodes / launches) if DRAM_BYTES_PER_NODE else None,
                      "kernel": f"ddg::batch_kernel<{solver.block_shape}>",
-                     "algorithmic_bytes": "TT bytes read+written per launch, counted in-kernel "
-                                          f"({tt_bytes / max(1, nodes):.1f} B/node)"},
-        "clocks": clocks,
-        "gpu_launches": len(stats),
+                     "algorithmic_bytes": (f"64 B per TT probe + 16 B per entry read + 80 B per store: "
+                                           f"{alg_bytes / max(1, nodes):.1f} B/node (the kernel's own count, which "
+                                           f"also charges each store its tag-line read: "
+                                           f"{counted / max(1, nodes):.1f} B/node)")},
+        "clocks": run["clocks"],
+        "gpu_launches": launches,
     }
     if e2e_ms:
-        line["e2e"] = {"value": e2e_jobs_all / JPD / (e2e_ms * 1e-3), "unit": "deals/s",
-                       "h2d_bytes_per_step": n * 32, "d2h_bytes_per_step": n * 20}
+        e2e_cost = costs.get(head) if (head == "plain" or guided_cost_ok) else None
+        e2e_val = (e2e_nodes_all / (e2e_ms_all * 1e-3) / e2e_cost["nodes_per_deal"]) if e2e_cost else None
+        line["e2e"] = {"value": e2e_val if e2e_val is not None else e2e_jobs / JPD / (e2e_ms * 1e-3),
+                       "unit": "deals/s", "h2d_bytes_per_step": n * 32, "d2h_bytes_per_step": n * 20}
     if cpu:
-        line["cpu_baseline"] = cpu
+        line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        line["cpu_baseline"].update({"nodes_per_s": cpu["nodes_per_s"],
+                                     "finished_deals_per_s": cpu["finished_deals_per_s"], "job_ms": cpu["job_ms"]})
+        line["vs_cpu_nodes_per_s"] = s_head["nodes_per_s"] / cpu["nodes_per_s"] if cpu["nodes_per_s"] else None
     print(json.dumps(line), flush=True)
     solver.close()
 
 
-def main():
-    a = parse()
+def main(argv=None):
+    argv = sys.argv[1:] if argv is None else argv
+    a = parse(argv)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    plan = launch_plan(a.gpus, os.environ)
+    if plan == "refuse":
+        print(f"bench.py: --gpus {a.gpus} but started as one of {world} ranks", file=sys.stderr)
+        return 2
+    if plan == "spawn":
+        return spawn_ranks(a.gpus, argv)
     if a.impl == "reference":
         reference_arm(a, rank, world)
-        return
+        return 0
     if world > 1:
         import datetime
         import torch
@@ -394,7 +542,8 @@ def main():
         if world > 1:
             import torch
             torch.distributed.destroy_process_group()
+    return 0
 
 
 if __name__ == "__main__":
-    main()
+    sys.exit(main())

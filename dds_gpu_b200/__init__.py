@@ -17,7 +17,10 @@ __all__ = ["Solver", "Stream", "Guide", "DDGError", "make_deals", "make_deals_mi
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "_lib", "libddg.so")
+# the same library built with bounds checks on every stack, TT and task index (tests)
+CHECK_LIB_PATH = os.path.join(_HERE, "_lib", "libddg_check.so")
 _lib = None
+_libs = {}
 
 
 class DDGError(RuntimeError):
@@ -43,7 +46,7 @@ class _Stats(ctypes.Structure):
                 ("tasks", ctypes.c_uint64),
                 ("jobs_done", ctypes.c_int64),
                 ("kernel_ms", ctypes.c_double), ("lanes", ctypes.c_int), ("grid", ctypes.c_int),
-                ("block", ctypes.c_int)]
+                ("block", ctypes.c_int), ("tt_entry_reads", ctypes.c_uint64)]
 
     def as_dict(self):
         d = {}
@@ -60,14 +63,18 @@ def library_path():
     return _LIB_PATH
 
 
-def load_library():
-    """Loads libddg.so (once). Raises DDGError when it has not been built."""
+def load_library(path=None):
+    """Loads libddg.so (once; `path` = another build of it, e.g. CHECK_LIB_PATH). Raises
+    DDGError when it has not been built."""
     global _lib
-    if _lib is not None:
+    if path is None and _lib is not None:
         return _lib
-    if not os.path.exists(_LIB_PATH):
-        raise DDGError(f"{_LIB_PATH} is missing: build it with `python -m dds_gpu_b200.build`")
-    lib = ctypes.CDLL(_LIB_PATH)
+    path = path or _LIB_PATH
+    if path in _libs:
+        return _libs[path]
+    if not os.path.exists(path):
+        raise DDGError(f"{path} is missing: build it with `python -m dds_gpu_b200.build`")
+    lib = ctypes.CDLL(path)
     lib.ddg_version.restype = ctypes.c_char_p
     lib.ddg_last_error.restype = ctypes.c_char_p
     lib.ddg_config_default.argtypes = [ctypes.POINTER(_Config)]
@@ -79,6 +86,7 @@ def load_library():
     lib.ddg_solver_nodes.argtypes = [P]
     lib.ddg_solver_nodes.restype = ctypes.c_uint64
     lib.ddg_solver_set_job_times.argtypes = [P, P]
+    lib.ddg_solver_set_job_starts.argtypes = [P, P]
     lib.ddg_solve_batch.argtypes = [P, P, ctypes.c_int64, P, ctypes.POINTER(_Stats)]
     lib.ddg_solve_batch_seeded.argtypes = [P, P, ctypes.c_int64, P, P, ctypes.POINTER(_Stats)]
     lib.ddg_solve_device.argtypes = [P, P, ctypes.c_int64, P, P, P, P, ctypes.POINTER(_Stats)]
@@ -89,6 +97,8 @@ def load_library():
     lib.ddg_solve_continue.argtypes = [P, ctypes.c_double, P, P, P, ctypes.POINTER(_Stats),
                                        ctypes.POINTER(ctypes.c_int)]
     lib.ddg_solve_strain.argtypes = [P, P, ctypes.c_int, P, P]
+    lib.ddg_ns_tricks.argtypes = [P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                  ctypes.POINTER(ctypes.c_int)]
     lib.ddg_stream_open.argtypes = [P, ctypes.c_int, ctypes.c_double, ctypes.POINTER(P)]
     lib.ddg_stream_submit.argtypes = [P, P, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]
     lib.ddg_stream_poll.argtypes = [P, P, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]
@@ -111,13 +121,16 @@ def load_library():
     lib.ddg_make_deals_mixed.argtypes = [ctypes.c_uint64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int, ctypes.c_int,
                                          ctypes.c_double, P]
     lib.ddg_make_deals_mixed.restype = None
-    _lib = lib
+    _libs[path] = lib
+    if path == _LIB_PATH:
+        _lib = lib
     return lib
 
 
-def _check(rc):
+def _check(last_error, rc):
+    """Raises DDGError with the library's message (its own ddg_last_error) for rc != 0."""
     if rc != 0:
-        raise DDGError(f"ddg error {rc}: {load_library().ddg_last_error().decode()}")
+        raise DDGError(f"ddg error {rc}: {last_error().decode()}")
 
 
 def make_deals(seed, first, n, k=13):
@@ -147,8 +160,8 @@ class Solver:
 
     def __init__(self, tt_log2=10, lanes=0, block=0, jobs_per_deal=5, device=0, schedule=0,
                  time_limit_s=0.0, mem_fraction=0.85, min_blocks=0, help=0, free_below=0, free_steps=0,
-                 phase_spread=0, cheap_limit=0):
-        lib = load_library()
+                 phase_spread=0, cheap_limit=0, library=None):
+        lib = library or load_library()
         cfg = _Config()
         lib.ddg_config_default(ctypes.byref(cfg))
         cfg.tt_log2, cfg.lanes, cfg.block = tt_log2, lanes, block
@@ -161,7 +174,7 @@ class Solver:
         cfg.time_limit_s, cfg.mem_fraction = time_limit_s, mem_fraction
         self._lib = lib
         self._h = P()
-        _check(lib.ddg_solver_create(ctypes.byref(cfg), ctypes.byref(self._h)))
+        _check(lib.ddg_last_error, lib.ddg_solver_create(ctypes.byref(cfg), ctypes.byref(self._h)))
         self.config = {name: getattr(cfg, name) for name, _ in cfg._fields_}
         blk = block or 512
         self.block_shape = f"{blk}, {min_blocks or (2 if blk == 256 else 1)}"
@@ -195,10 +208,10 @@ class Solver:
         out = np.empty((n, 5, 4), dtype=np.uint8)
         st = _Stats()
         if seeds is None:
-            _check(self._lib.ddg_solve_batch(self._h, h.ctypes.data, n, out.ctypes.data, ctypes.byref(st)))
+            _check(self._lib.ddg_last_error, self._lib.ddg_solve_batch(self._h, h.ctypes.data, n, out.ctypes.data, ctypes.byref(st)))
         else:
             sd = np.ascontiguousarray(seeds, dtype=np.int8).reshape(n, 20)
-            _check(self._lib.ddg_solve_batch_seeded(self._h, h.ctypes.data, n, sd.ctypes.data,
+            _check(self._lib.ddg_last_error, self._lib.ddg_solve_batch_seeded(self._h, h.ctypes.data, n, sd.ctypes.data,
                                                     out.ctypes.data, ctypes.byref(st)))
         self.last_stats = st.as_dict()
         return out
@@ -207,7 +220,7 @@ class Solver:
         """Device-pointer form (ddg_solve_device / _ex): integer addresses of device buffers;
         d_hints / d_best = the guide's root leads in and best leads out (n*20 int8)."""
         st = _Stats()
-        _check(self._lib.ddg_solve_device_ex(self._h, P(d_hands), n, P(d_seeds or None), P(d_hints or None),
+        _check(self._lib.ddg_last_error, self._lib.ddg_solve_device_ex(self._h, P(d_hands), n, P(d_seeds or None), P(d_hints or None),
                                              P(d_out), P(d_best or None), P(d_job_nodes or None),
                                              P(stream or None), ctypes.byref(st)))
         self.last_stats = st.as_dict()
@@ -215,7 +228,7 @@ class Solver:
 
     def begin(self, d_hands, n, d_out, d_seeds=0, stream=0, d_hints=0):
         """Starts a resumable solve on device buffers (ddg_solve_begin_ex)."""
-        _check(self._lib.ddg_solve_begin_ex(self._h, P(d_hands), n, P(d_seeds or None), P(d_hints or None),
+        _check(self._lib.ddg_last_error, self._lib.ddg_solve_begin_ex(self._h, P(d_hands), n, P(d_seeds or None), P(d_hints or None),
                                             P(d_out), P(stream or None)))
 
     def resume(self, seconds, hands_host=0, out_host=0, stream=0):
@@ -223,7 +236,7 @@ class Solver:
         (finished, stats of the slice)."""
         st = _Stats()
         fin = ctypes.c_int(0)
-        _check(self._lib.ddg_solve_continue(self._h, seconds, P(hands_host or None), P(out_host or None),
+        _check(self._lib.ddg_last_error, self._lib.ddg_solve_continue(self._h, seconds, P(hands_host or None), P(out_host or None),
                                             P(stream or None), ctypes.byref(st), ctypes.byref(fin)))
         self.last_stats = st.as_dict()
         return bool(fin.value), self.last_stats
@@ -231,23 +244,35 @@ class Solver:
     def solve_graph(self, d_hands, n, d_out, d_seeds=0, stream=0):
         """The batch solve as a replayed CUDA graph (ddg_solve_graph)."""
         st = _Stats()
-        _check(self._lib.ddg_solve_graph(self._h, P(d_hands), n, P(d_seeds or None), P(d_out), P(stream or None),
+        _check(self._lib.ddg_last_error, self._lib.ddg_solve_graph(self._h, P(d_hands), n, P(d_seeds or None), P(d_out), P(stream or None),
                                          ctypes.byref(st)))
         self.last_stats = st.as_dict()
         return self.last_stats
 
-    def set_job_times(self, d_job_end_ns):
-        """Device buffer (integer address, n*jobs_per_deal uint64) for job completion times."""
-        _check(self._lib.ddg_solver_set_job_times(self._h, P(d_job_end_ns or None)))
+    def set_job_times(self, d_job_end_ns, d_job_start_ns=None):
+        """Device buffers (integer addresses, n*jobs_per_deal uint64) for job completion
+        times and, when given, the times the jobs were taken (0 = unused)."""
+        _check(self._lib.ddg_last_error, self._lib.ddg_solver_set_job_times(self._h, P(d_job_end_ns or None)))
+        if d_job_start_ns is not None:
+            _check(self._lib.ddg_last_error, self._lib.ddg_solver_set_job_starts(self._h, P(d_job_start_ns or None)))
 
     def solve_strain(self, hands4, strain, ns4=None):
         """One strain of one deal, declarers N,E,S,W (the reference's dd_solve_strain)."""
         h = np.ascontiguousarray(hands4, dtype=np.uint64).reshape(4)
         out = np.zeros(4, dtype=np.int32)
         s4 = None if ns4 is None else np.ascontiguousarray(ns4, dtype=np.int32)
-        _check(self._lib.ddg_solve_strain(self._h, h.ctypes.data, strain,
+        _check(self._lib.ddg_last_error, self._lib.ddg_solve_strain(self._h, h.ctypes.data, strain,
                                           None if s4 is None else s4.ctypes.data, out.ctypes.data))
         return [int(x) for x in out]
+
+    def ns_tricks(self, hands4, strain, leader, guess=7, stepping=False):
+        """NS tricks with `leader` on lead (the reference's dd_ns_tricks, or dd_ns_tricks_from
+        with stepping=True, starting at `guess`)."""
+        h = np.ascontiguousarray(hands4, dtype=np.uint64).reshape(4)
+        v = ctypes.c_int(0)
+        _check(self._lib.ddg_last_error, self._lib.ddg_ns_tricks(self._h, h.ctypes.data, strain, leader, guess, 1 if stepping else 0,
+                                       ctypes.byref(v)))
+        return v.value
 
 
 class Stream:
@@ -257,7 +282,7 @@ class Stream:
     def __init__(self, solver, ring_slots=0, idle_timeout_s=0.0):
         self._lib = solver._lib
         self._h = P()
-        _check(self._lib.ddg_stream_open(solver._h, ring_slots, idle_timeout_s, ctypes.byref(self._h)))
+        _check(self._lib.ddg_last_error, self._lib.ddg_stream_open(solver._h, ring_slots, idle_timeout_s, ctypes.byref(self._h)))
         self.stats = None
 
     @property
@@ -272,14 +297,14 @@ class Stream:
         """Submits deals (n, 4) uint64 in order; returns how many were admitted (a prefix)."""
         h = np.ascontiguousarray(hands, dtype=np.uint64).reshape(-1, 4)
         acc = ctypes.c_int64(0)
-        _check(self._lib.ddg_stream_submit(self._h, h.ctypes.data, h.shape[0], ctypes.byref(acc)))
+        _check(self._lib.ddg_last_error, self._lib.ddg_stream_submit(self._h, h.ctypes.data, h.shape[0], ctypes.byref(acc)))
         return acc.value
 
     def poll(self, max_records=65536):
         """Finished deals: (indices uint64 (k,), tricks uint8 (k, 5, 4))."""
         buf = np.empty(max_records * 28, dtype=np.uint8)
         got = ctypes.c_int64(0)
-        _check(self._lib.ddg_stream_poll(self._h, buf.ctypes.data, max_records, ctypes.byref(got)))
+        _check(self._lib.ddg_last_error, self._lib.ddg_stream_poll(self._h, buf.ctypes.data, max_records, ctypes.byref(got)))
         rec = buf[: got.value * 28].reshape(-1, 28)
         return rec[:, :8].copy().view(np.uint64).reshape(-1), rec[:, 8:].reshape(-1, 5, 4).copy()
 
@@ -288,7 +313,7 @@ class Stream:
         if self._h:
             st = _Stats()
             h, self._h = self._h, P()
-            _check(self._lib.ddg_stream_close(h, 1 if drain else 0, ctypes.byref(st)))
+            _check(self._lib.ddg_last_error, self._lib.ddg_stream_close(h, 1 if drain else 0, ctypes.byref(st)))
             self.stats = st.as_dict()
         return self.stats
 
@@ -311,7 +336,7 @@ class Guide:
             p = np.ascontiguousarray(params, dtype=np.float32).reshape(-1)
             if p.size != self.param_count():
                 raise DDGError(f"guide parameters: {p.size} values, {self.param_count()} expected")
-        _check(self._lib.ddg_guide_create(device, max_rows, p.ctypes.data if p is not None else None,
+        _check(self._lib.ddg_last_error, self._lib.ddg_guide_create(device, max_rows, p.ctypes.data if p is not None else None,
                                           ctypes.byref(self._h)))
         self.max_rows = max_rows
 
@@ -332,12 +357,12 @@ class Guide:
 
     def params(self):
         out = np.empty(self.param_count(), dtype=np.float32)
-        _check(self._lib.ddg_guide_get_params(self._h, out.ctypes.data))
+        _check(self._lib.ddg_last_error, self._lib.ddg_guide_get_params(self._h, out.ctypes.data))
         return out
 
     def set_params(self, params):
         p = np.ascontiguousarray(params, dtype=np.float32).reshape(-1)
-        _check(self._lib.ddg_guide_set_params(self._h, p.ctypes.data))
+        _check(self._lib.ddg_last_error, self._lib.ddg_guide_set_params(self._h, p.ctypes.data))
 
     def step(self, d_hands, d_tricks20, d_best20, rows, lr, want_grad=False):
         """One training step on example indices `rows` (deal*20 + strain*4 + declarer);
@@ -345,10 +370,10 @@ class Guide:
         r = np.ascontiguousarray(rows, dtype=np.int64)
         stats = np.zeros(3, dtype=np.float32)
         grad = np.empty(self.param_count(), dtype=np.float32) if want_grad else None
-        _check(self._lib.ddg_guide_train_step(self._h, P(d_hands), P(d_tricks20), P(d_best20), r.ctypes.data,
+        _check(self._lib.ddg_last_error, self._lib.ddg_guide_train_step(self._h, P(d_hands), P(d_tricks20), P(d_best20), r.ctypes.data,
                                               r.size, lr, stats.ctypes.data,
                                               grad.ctypes.data if grad is not None else None))
         return float(stats[0]), float(stats[1]), float(stats[2]), grad
 
     def predict(self, d_hands, n, d_seed20=0, d_hint20=0):
-        _check(self._lib.ddg_guide_predict(self._h, P(d_hands), n, P(d_seed20 or None), P(d_hint20 or None)))
+        _check(self._lib.ddg_last_error, self._lib.ddg_guide_predict(self._h, P(d_hands), n, P(d_seed20 or None), P(d_hint20 or None)))

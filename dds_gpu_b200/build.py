@@ -1,6 +1,6 @@
 """Builds the solver library and command-line tools in-tree (dds_gpu_b200/_lib/).
 
-    python -m dds_gpu_b200.build            # libddg.so, dd_gpu, dd_stream
+    python -m dds_gpu_b200.build            # libddg.so, libddg_check.so, dd_gpu, dd_stream
     python -m dds_gpu_b200.build --force    # rebuild even when up to date
 
 nvcc compiles for sm_100a only (-gencode arch=compute_100a,code=sm_100a); the output
@@ -24,6 +24,8 @@ NVFLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-I" 
 # target -> (sources, extra flags, kind)
 TARGETS = {
     "libddg.so": (["ddg_api.cu"], ["-shared"], "lib"),
+    # the same library with every stack, TT and task index checked before use (tests)
+    "libddg_check.so": (["ddg_api.cu"], ["-shared", "-DDDG_BOUNDS_CHECK"], "lib"),
 }
 CLI = {
     "dd_gpu": "cli_dd_gpu.cpp",

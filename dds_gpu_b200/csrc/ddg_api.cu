@@ -59,6 +59,7 @@ struct ddg_solver {
   int64_t cap = 0;
   uint64_t total_nodes = 0;  // search nodes over all calls
   uint64_t* d_job_end_ns = nullptr;  // caller's buffer for job completion times, or null
+  uint64_t* d_job_start_ns = nullptr;  // caller's buffer for the times jobs were taken, or null
   uint64_t start_ns = 0;             // device global timer at the last solve's launch
   TaskPool* tasks = nullptr;         // helping's task pool (cfg.help), cleared per solve
   // Resumable (time-sliced) solve.
@@ -69,14 +70,18 @@ struct ddg_solver {
   bool streaming = false;  // a ddg_stream owns the lanes until it is closed
   // CUDA graph of one batch solve (ddg_solve_graph): rebuilt when its arguments change.
   cudaGraphExec_t graph = nullptr;
-  const void* graph_key[4] = {nullptr, nullptr, nullptr, nullptr};
+  const void* graph_key[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   int64_t graph_n = -1;
   int graph_grid = 0;
 };
 
 extern "C" {
 
-const char* ddg_version(void) { return "ddg 0.1 (sm_100a)"; }
+#ifdef DDG_BOUNDS_CHECK
+const char* ddg_version(void) { return "ddg 0.2 (sm_100a, bounds-checked)"; }
+#else
+const char* ddg_version(void) { return "ddg 0.2 (sm_100a)"; }
+#endif
 const char* ddg_last_error(void) { return g_err; }
 
 void ddg_config_default(ddg_config* c) {
@@ -266,6 +271,12 @@ int ddg_solver_set_job_times(ddg_solver* s, uint64_t* d_job_end_ns) {
   s->d_job_end_ns = d_job_end_ns;
   return DDG_OK;
 }
+
+int ddg_solver_set_job_starts(ddg_solver* s, uint64_t* d_job_start_ns) {
+  if (!s) return fail(DDG_E_ARG, "null solver");
+  s->d_job_start_ns = d_job_start_ns;
+  return DDG_OK;
+}
 uint64_t ddg_solver_nodes(const ddg_solver* s) { return s ? s->total_nodes : 0; }
 int64_t ddg_solver_bytes(const ddg_solver* s) { return s ? (int64_t)s->bytes : 0; }
 
@@ -306,6 +317,7 @@ static BatchArgs make_args(ddg_solver* s, const uint64_t* d_hands, int64_t n, co
   a.schedule = s->cfg.schedule;
   a.stop = s->d_stop;
   a.job_end_ns = s->d_job_end_ns;
+  a.job_start_ns = s->d_job_start_ns;
   a.tasks = s->tasks;
   a.free_below = s->cfg.free_below == 0 ? 64 : s->cfg.free_below < 0 ? 0 : s->cfg.free_below;
   a.free_steps = s->cfg.free_steps > 0 ? s->cfg.free_steps : 256;
@@ -322,12 +334,16 @@ static int read_stats(ddg_solver* s, int grid, ddg_stats* st, unsigned long long
   s->total_nodes += c[CNT_NODES];
   if (c[CNT_FAULTS])
     return fail(DDG_E_TIMEOUT, "%llu blocks gave up a bounded queue wait; results incomplete", c[CNT_FAULTS]);
+  if (c[CNT_BOUNDS])
+    return fail(DDG_E_STATE, "bounds check: %llu out-of-range accesses were skipped; results incomplete",
+                c[CNT_BOUNDS]);
   if (!st) return DDG_OK;
   st->nodes = c[CNT_NODES];
   st->tt_probes = c[CNT_PROBES];
   st->tt_hits = c[CNT_HITS];
   st->tt_stores = c[CNT_STORES];
   st->tt_bytes = c[CNT_TT_BYTES];
+  st->tt_entry_reads = c[CNT_ENTRY_READS];
   for (int k = 0; k < 7; k++) st->enter_exit[k] = c[CNT_EXIT + k];
   for (int k = 0; k < PH_COUNT; k++) {
     st->phase_warps[k] = c[CNT_PHASE_WARPS + k];
@@ -397,6 +413,7 @@ int ddg_solve_device_ex(ddg_solver* s, const uint64_t* d_hands, int64_t n, const
   *(volatile int*)s->h_stop = 0;
   if (s->tasks) CUDA_TRY(cudaMemsetAsync(s->tasks, 0, sizeof(TaskPool), stream));
   if (s->d_job_end_ns) CUDA_TRY(cudaMemsetAsync(s->d_job_end_ns, 0, (size_t)a.n_jobs * 8, stream));
+  if (s->d_job_start_ns) CUDA_TRY(cudaMemsetAsync(s->d_job_start_ns, 0, (size_t)a.n_jobs * 8, stream));
   CUDA_TRY(cudaEventRecord(s->ev0, stream));
   int grid = 0;
   int rc = launch_batch(s, a, a.n_jobs, stream, &grid);
@@ -419,7 +436,8 @@ int ddg_solve_graph(ddg_solver* s, const uint64_t* d_hands, int64_t n, const int
   s->sliced = false;
   cudaStream_t stream = (cudaStream_t)stream_v;
   const bool same = s->graph && s->graph_n == n && s->graph_key[0] == d_hands && s->graph_key[1] == d_seed20 &&
-                    s->graph_key[2] == d_out20 && s->graph_key[3] == s->d_job_end_ns;
+                    s->graph_key[2] == d_out20 && s->graph_key[3] == s->d_job_end_ns &&
+                    s->graph_key[4] == s->d_job_start_ns;
   if (!same) {
     if (s->graph) cudaGraphExecDestroy(s->graph);
     s->graph = nullptr;
@@ -428,6 +446,7 @@ int ddg_solve_graph(ddg_solver* s, const uint64_t* d_hands, int64_t n, const int
     CUDA_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
     BatchArgs a = make_args(s, d_hands, n, d_seed20, d_out20, nullptr);
     a.job_end_ns = s->d_job_end_ns;
+    a.job_start_ns = s->d_job_start_ns;
     cudaGraph_t g = nullptr;
     int grid = 0, rc = DDG_OK;
     cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
@@ -435,6 +454,8 @@ int ddg_solve_graph(ddg_solver* s, const uint64_t* d_hands, int64_t n, const int
     if (e == cudaSuccess) e = cudaMemsetAsync(d_out20, 0xFF, (size_t)n * 20, cap);
     if (e == cudaSuccess && s->tasks) e = cudaMemsetAsync(s->tasks, 0, sizeof(TaskPool), cap);
     if (e == cudaSuccess && s->d_job_end_ns) e = cudaMemsetAsync(s->d_job_end_ns, 0, (size_t)a.n_jobs * 8, cap);
+    if (e == cudaSuccess && s->d_job_start_ns)
+      e = cudaMemsetAsync(s->d_job_start_ns, 0, (size_t)a.n_jobs * 8, cap);
     if (e == cudaSuccess) rc = launch_batch(s, a, a.n_jobs, cap, &grid);
     cudaError_t e2 = cudaStreamEndCapture(cap, &g);
     if (e == cudaSuccess) e = e2;
@@ -451,6 +472,7 @@ int ddg_solve_graph(ddg_solver* s, const uint64_t* d_hands, int64_t n, const int
     s->graph_key[1] = d_seed20;
     s->graph_key[2] = d_out20;
     s->graph_key[3] = s->d_job_end_ns;
+    s->graph_key[4] = s->d_job_start_ns;
     s->graph_grid = grid;
   }
   *(volatile int*)s->h_stop = 0;
@@ -494,6 +516,8 @@ int ddg_solve_begin_ex(ddg_solver* s, const uint64_t* d_hands, int64_t n, const 
   CUDA_TRY(cudaMemsetAsync(d_out20, 0xFF, (size_t)n * 20, stream));
   if (s->tasks) CUDA_TRY(cudaMemsetAsync(s->tasks, 0, sizeof(TaskPool), stream));
   if (s->d_job_end_ns) CUDA_TRY(cudaMemsetAsync(s->d_job_end_ns, 0, (size_t)s->slice_args.n_jobs * 8, stream));
+  if (s->d_job_start_ns)
+    CUDA_TRY(cudaMemsetAsync(s->d_job_start_ns, 0, (size_t)s->slice_args.n_jobs * 8, stream));
   s->sliced = true;
   s->slice_done = false;
   return DDG_OK;
@@ -596,6 +620,7 @@ static int stream_kernel(ddg_stream* st) {
   BatchArgs a = make_args(s, nullptr, 0, nullptr, st->d_out, nullptr);
   a.tasks = nullptr;  // lanes without a deal wait for the next one instead of helping
   a.job_end_ns = nullptr;
+  a.job_start_ns = nullptr;
   a.ring = st->d_ring;
   a.published = st->d_words + 0;
   a.next_job = st->d_words + 1;
@@ -828,18 +853,75 @@ int ddg_solve_batch_seeded(ddg_solver* s, const uint64_t* hands, int64_t n, cons
   return solve_host(s, hands, n, ns_seed20, out20, st);
 }
 
-int ddg_solve_strain(ddg_solver* s, const uint64_t* hands4, int strain, const int* ns4, int* out4) {
+// One job of one deal: strain `strain` for declarer `decl` (or all four, decl = -1), with
+// seeds (stepping search) or a first target (binary search). out20 receives the deal's
+// table row of that strain. The calls for one strain or one lead of the reference's API.
+static int solve_one(ddg_solver* s, const uint64_t* hands4, int strain, int decl, const int8_t* seeds20,
+                     int first_target, uint8_t* out20) {
+  if (!s) return fail(DDG_E_ARG, "null solver");
+  if (!hands4 || !out20) return fail(DDG_E_ARG, "null argument");
   if (strain < 0 || strain > 4) return fail(DDG_E_ARG, "strain %d is not 0..4", strain);
+  if (s->streaming) return fail(DDG_E_STATE, "a stream is open on this solver");
+  int rc = ddg_check_deal(hands4);
+  if (rc) return rc;
+  CUDA_TRY(cudaSetDevice(s->device));
+  rc = ensure_staging(s, 1);
+  if (rc) return rc;
+  s->sliced = false;
+  CUDA_TRY(cudaMemcpy(s->d_hands, hands4, 32, cudaMemcpyHostToDevice));
+  if (seeds20) CUDA_TRY(cudaMemcpy(s->d_seeds, seeds20, 20, cudaMemcpyHostToDevice));
+  BatchArgs a = make_args(s, s->d_hands, 1, seeds20 ? s->d_seeds : nullptr, s->d_out, nullptr);
+  a.n_jobs = 1;
+  a.one_job = 1;
+  a.one_strain = strain;
+  a.one_decl = decl;
+  a.first_target = first_target;
+  CUDA_TRY(cudaMemset(s->counters, 0, CNT_WORDS * 8));
+  CUDA_TRY(cudaMemset(s->d_out, 0xFF, 20));
+  if (s->tasks) CUDA_TRY(cudaMemset(s->tasks, 0, sizeof(TaskPool)));
+  *(volatile int*)s->h_stop = 0;
+  CUDA_TRY(cudaEventRecord(s->ev0, nullptr));
+  int grid = 0;
+  rc = launch_batch(s, a, 1, nullptr, &grid);
+  if (rc) return rc;
+  CUDA_TRY(cudaEventRecord(s->ev1, nullptr));
+  rc = wait_launch(s);
+  if (rc) return rc;
+  unsigned long long c[CNT_WORDS];
+  rc = read_stats(s, grid, nullptr, c);
+  if (rc) return rc;
+  CUDA_TRY(cudaMemcpy(out20, s->d_out, 20, cudaMemcpyDeviceToHost));
+  return DDG_OK;
+}
+
+int ddg_solve_strain(ddg_solver* s, const uint64_t* hands4, int strain, const int* ns4, int* out4) {
   if (!out4) return fail(DDG_E_ARG, "null output");
   int8_t seeds[20];
   for (int i = 0; i < 20; i++) seeds[i] = 7;
-  if (ns4)
+  if (ns4 && strain >= 0 && strain <= 4)
     for (int d = 0; d < 4; d++) seeds[strain * 4 + d] = (int8_t)ns4[d];
   uint8_t out[20];
-  // One deal: all five strains are solved; the batch form amortises this.
-  int rc = solve_host(s, hands4, 1, ns4 ? seeds : nullptr, out, nullptr);
+  int rc = solve_one(s, hands4, strain, -1, ns4 ? seeds : nullptr, 0, out);
   if (rc) return rc;
   for (int d = 0; d < 4; d++) out4[d] = out[strain * 4 + d];
+  return DDG_OK;
+}
+
+int ddg_ns_tricks(ddg_solver* s, const uint64_t* hands4, int strain, int leader, int guess, int stepping,
+                  int* ns_out) {
+  if (!ns_out) return fail(DDG_E_ARG, "null output");
+  if (leader < 0 || leader > 3) return fail(DDG_E_ARG, "leader %d is not 0..3", leader);
+  const int decl = (leader + 3) & 3;
+  int8_t seeds[20];
+  for (int i = 0; i < 20; i++) seeds[i] = (int8_t)(guess < -1 ? -1 : guess > 13 ? 13 : guess);
+  uint8_t out[20];
+  // The binary search clamps its first target to 1..13 (src/dd.h:881); the stepping
+  // search clamps its seed to 0..tricks left (src/dd.h:903).
+  const int first = guess < 1 ? 1 : guess > 13 ? 13 : guess;
+  int rc = solve_one(s, hands4, strain, decl, stepping ? seeds : nullptr, stepping ? 0 : first, out);
+  if (rc) return rc;
+  const int v = out[strain * 4 + decl];
+  *ns_out = (decl & 1) == 0 ? v : 13 - v;
   return DDG_OK;
 }
 

@@ -17,8 +17,6 @@
 
 namespace ddg {
 
-enum { STACK_DEPTH = 54 };  // frames per lane: at most 52 plies + the root
-
 // Device statistics block (u64 words).
 enum {
   CNT_NEXT_JOB = 0,
@@ -36,7 +34,9 @@ enum {
   CNT_PHASE_CYCLES = 32,  // 8 words: SM cycles per phase, summed over blocks
   CNT_FAULTS = 38,        // blocks whose bounded queue wait gave up (never expected)
   CNT_BLOCKS_DONE = 39,   // blocks that ended with every lane idle (the solve is complete)
-  CNT_WORDS = 40
+  CNT_BOUNDS = 40,        // bounds-checked builds: out-of-range accesses skipped (never expected)
+  CNT_ENTRY_READS = 41,   // TT entries read by probes
+  CNT_WORDS = 42
 };
 
 struct BatchArgs {
@@ -55,6 +55,7 @@ struct BatchArgs {
   int schedule;
   volatile int* stop;    // host-set stop flag (mapped memory), or null
   u64* job_end_ns;       // n * jpd completion times (device global timer, ns), or null
+  u64* job_start_ns;     // n * jpd times the jobs were taken by a lane, or null
   TaskPool* tasks;       // helping: idle lanes take donated moves (tricks exact), or null
   int free_below;        // fewer busy lanes than this in a block: each thread runs its own lane
   int free_steps;        // stages a lane runs per free-running round
@@ -77,6 +78,10 @@ struct BatchArgs {
   int fuse_follow;       // ENTER inside a trick runs in the cheap pass (no FOLLOW phase)
   const int8_t* hint20;  // n * 20 root leads to try first (learned guide), -1 = none; or null
   int8_t* best20;        // n * 20 best leads found (the cutting root card), -1 = none; or null
+  // One-job solves (ddg_solve_strain, ddg_ns_tricks): with `one_job` set, job 0 is strain
+  // `one_strain` of deal 0, for declarer `one_decl` alone (-1 = all four). A zeroed
+  // BatchArgs has it off. `first_target` is the binary search's first target (0 = 7).
+  int one_job, one_strain, one_decl, first_target;
 };
 
 // One finished deal of a stream: its sequence number and table; `flag` = record index + 1,
@@ -215,8 +220,14 @@ struct DevEnv {
       L.decl = sub & 3;
       L.last_decl = L.decl;
     }
+    if (a->one_job) {
+      L.strain = a->one_strain;
+      L.decl = a->one_decl >= 0 ? a->one_decl : 0;
+      L.last_decl = a->one_decl >= 0 ? a->one_decl : 3;
+    }
     L.mode = a->mode;
     c->start_nodes = c->s.nodes;
+    if (a->job_start_ns) a->job_start_ns[L.job] = global_ns();
     return 1;
   }
   // Stream: claims the next published job, if any.
@@ -241,7 +252,8 @@ struct DevEnv {
     return (long long)*reinterpret_cast<volatile unsigned long long*>(a->next_job) < avail;
   }
   __device__ __forceinline__ int seed(const Lane& L) {
-    return a->mode == MODE_STEP ? (int)a->seeds[L.deal * 20 + L.strain * 4 + L.decl] : 7;
+    if (a->mode == MODE_STEP) return (int)a->seeds[L.deal * 20 + L.strain * 4 + L.decl];
+    return a->first_target ? a->first_target : 7;
   }
   __device__ __forceinline__ long long out_row(const Lane& L) const {
     return a->ring ? (L.deal & a->ring_mask) : L.deal;
@@ -272,9 +284,11 @@ struct DevEnv {
     volatile CompRec* r = a->comp + (idx & (unsigned long long)a->ring_mask);
     r->seq = (unsigned long long)L.deal;
     for (int k = 0; k < 20; k++) r->tricks[k] = o[k];
-    __threadfence_system();  // the record before its flag
-    r->flag = (unsigned)idx + 1u;
+    // The slot's count is reset before the flag lets the host free the slot: a job of the
+    // next deal in this slot must not find the old count.
     a->deal_done[slot] = 0;
+    __threadfence_system();  // the record and the reset before the flag
+    r->flag = (unsigned)idx + 1u;
   }
 };
 
@@ -721,6 +735,8 @@ __device__ __forceinline__ void block_counters(BlockShared<BLOCK>& sh, const Bat
         case CNT_STORES: sum += c.s.tt.stores; break;
         case CNT_TT_BYTES: sum += c.s.tt.bytes; break;
         case CNT_JOBS_DONE: sum += c.jobs_done; break;
+        case CNT_BOUNDS: sum += c.s.bounds; break;
+        case CNT_ENTRY_READS: sum += c.s.tt.entry_reads; break;
         default:
           if (tid >= CNT_EXIT && tid < CNT_EXIT + 7) sum += c.s.enter_exit[tid - CNT_EXIT];
       }

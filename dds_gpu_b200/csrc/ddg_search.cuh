@@ -90,7 +90,26 @@ struct LaneStats {
   u64 nodes;
   TTStats tt;
   u32 enter_exit[7];  // trivial, last trick, TT hit, quick tricks, later tricks, QT 2nd hand, expanded
+  u32 bounds;         // bounds-checked builds: accesses out of range, skipped
 };
+
+// Frames per lane: the root and at most 52 plies below it, plus one spare (the reference's
+// dd_search keeps 53 frames, src/dd.h:802).
+#ifndef DDG_STACK_DEPTH
+#define DDG_STACK_DEPTH 54
+#endif
+enum { STACK_DEPTH = DDG_STACK_DEPTH };
+
+// Bounds-checked builds (-DDDG_BOUNDS_CHECK, libddg_check.so): every frame-stack index,
+// TT bucket index and task index is checked before its access; a check that fails counts
+// in LaneStats::bounds, the access is skipped and the lane stops (its results stay
+// unsolved, and the call reports the count as an error). It never traps: the device and
+// the context stay usable. In the default build the checks compile to nothing.
+#ifdef DDG_BOUNDS_CHECK
+#define DDG_IN_BOUNDS(cond, st) ((cond) || ((st).bounds++, false))
+#else
+#define DDG_IN_BOUNDS(cond, st) true
+#endif
 
 DDG_HD int trick_at(const Pos& p, int i) { return trick_card(p.trick, i); }
 
@@ -225,6 +244,7 @@ DDG_CALL int enter_lead(Pos& p, int target, Frame& f, u64& rel, Top& top, TTBuck
   Hands hs;
   for (int i = 0; i < 4; i++) hs.h[i] = p.h[i];
   const NodeKey key = make_key(hs, p.leader, p.left, gen, mask);
+  if (!DDG_IN_BOUNDS(key.bucket <= mask, st)) return 0;
   const ProbeOut pr = tt_probe(tt, key, need, st.tt);
   if (pr.hit >= 0) {
     rel = pr.rel;
@@ -345,7 +365,7 @@ DDG_CALL u64 finish(const Pos& p, const Frame& f, TTBucket* tt, u32 mask, u32 ge
     Hands hs;
     for (int i = 0; i < 4; i++) hs.h[i] = p.h[i];
     const NodeKey key = make_key(hs, p.leader, p.left, gen, mask);
-    tt_store(tt, key, gen, acc, lb, ub, fr_best(f), st.tt);
+    if (DDG_IN_BOUNDS(key.bucket <= mask, st)) tt_store(tt, key, gen, acc, lb, ub, fr_best(f), st.tt);
   }
   return acc;
 }
@@ -639,6 +659,10 @@ DDG_HD int root_result(Lane& L) {
 template <class Env>
 DDG_CALL void node_done(Lane& L, Env& env) {
   if (L.sp > 0) {
+    if (!DDG_IN_BOUNDS(L.sp <= STACK_DEPTH, env.stats())) {
+      L.stage = ST_IDLE;
+      return;
+    }
     L.sp--;
     if (L.par_sp == L.sp) L.f = L.par;  // the frame pushed last: still in shared memory
     else frame_load(L.f, env.stack + L.sp);
@@ -776,6 +800,10 @@ template <class Env>
 DDG_CALL void frame_done(Lane& L, Env& env) {
   Frame& f = L.f;
   if (L.sp == 0 && L.task >= 0) {
+    if (!DDG_IN_BOUNDS(L.task < MAX_TASKS, env.stats())) {
+      L.stage = ST_IDLE;
+      return;
+    }
     TaskPool& tp = *env.pool();
     task_finish(tp, L.task, L.v, f.acc, fr_best(f));
     L.task = -1;
@@ -795,6 +823,10 @@ DDG_CALL void step_next(Lane& L, Env& env) {
   for (;;) {
     int i = fr_i(f);
     const int n = fr_n(f);
+    if (!DDG_IN_BOUNDS(n <= 13 && L.sp < STACK_DEPTH, env.stats())) {
+      L.stage = ST_IDLE;
+      return;
+    }
     while (i < n) {
       int card = fr_move(f, i);
       int s = card_suit(card);
@@ -820,6 +852,10 @@ DDG_CALL void step_next(Lane& L, Env& env) {
     fr_set_i(f, i);
     const int t = fr_task(f);
     if (t < 0) break;
+    if (!DDG_IN_BOUNDS(t < MAX_TASKS, env.stats())) {
+      L.stage = ST_IDLE;
+      return;
+    }
     // Own children done; the donated tail decides what comes next.
     TaskPool& tp = *env.pool();
     if (task_retract(tp, t)) {  // nobody took it: search it here after all
@@ -857,7 +893,7 @@ DDG_CALL void step_ret(Lane& L, Env& env) {
   unplay(L.p, f, card, L.r);
   if (L.v == (int)ns_side(fr_seat(f))) {  // the child cuts
     const int t = fr_task(f);
-    if (t >= 0) {  // the donated tail is not needed any more
+    if (t >= 0 && DDG_IN_BOUNDS(t < MAX_TASKS, env.stats())) {  // the donated tail is not needed any more
       task_abandon(*env.pool(), t);
       fr_clear_task(f);
     }
@@ -875,6 +911,10 @@ DDG_CALL void step_ret(Lane& L, Env& env) {
 // WAIT: the top frame's donated tail is running on a helper.
 template <class Env>
 DDG_HD bool step_wait(Lane& L, Env& env) {
+  if (!DDG_IN_BOUNDS(fr_task(L.f) >= 0 && fr_task(L.f) < MAX_TASKS, env.stats())) {
+    L.stage = ST_IDLE;
+    return false;
+  }
   if (atom_load(&env.pool()->state[fr_task(L.f)]) != TASK_DONE) return false;
   L.stage = ST_NEXT;  // NEXT merges the result and finishes the frame
   return true;
@@ -926,15 +966,20 @@ DDG_CALL bool step_hungry(Lane& L, Env& env) {
 template <class Env>
 DDG_CALL void abort_task(Lane& L, Env& env) {
   TaskPool& tp = *env.pool();
+  if (!DDG_IN_BOUNDS(L.sp <= STACK_DEPTH && L.task >= 0 && L.task < MAX_TASKS, env.stats())) {
+    L.stage = ST_IDLE;
+    return;
+  }
   for (int k = 0; k < L.sp; k++) {
     Frame g;
     frame_load(g, env.stack + k);
-    if (fr_task(g) >= 0) task_abandon(tp, fr_task(g));
+    if (fr_task(g) >= 0 && DDG_IN_BOUNDS(fr_task(g) < MAX_TASKS, env.stats())) task_abandon(tp, fr_task(g));
   }
   // In NEXT, RET and WAIT the top frame is the one at depth sp; in ENTER and MOVES it is
   // the copy of frame sp-1 (done above) or a fresh frame without a task.
   const bool top_is_own = L.stage == ST_NEXT || L.stage == ST_RET || L.stage == ST_WAIT;
-  if (top_is_own && fr_task(L.f) >= 0) task_abandon(tp, fr_task(L.f));
+  if (top_is_own && fr_task(L.f) >= 0 && DDG_IN_BOUNDS(fr_task(L.f) < MAX_TASKS, env.stats()))
+    task_abandon(tp, fr_task(L.f));
   tp.state[L.task] = TASK_FREE;
   L.task = -1;
   atom_add(&tp.busy, -1);
@@ -950,6 +995,7 @@ DDG_HD bool task_abandoned(const Lane& L, const TaskPool* tp) {
 // frame; the donated frame's position is found by taking back the moves above it.
 template <class Env>
 DDG_CALL bool try_donate(Lane& L, Env& env) {
+  if (!DDG_IN_BOUNDS(L.sp <= STACK_DEPTH, env.stats())) return false;
   const int top = L.sp < MAX_DONATE_DEPTH ? L.sp : MAX_DONATE_DEPTH;
   for (int d = 0; d < top; d++) prefetch_l1(env.stack + d);  // the scan's loads, in flight together
   for (int d = 0; d < top; d++) {

@@ -3,8 +3,10 @@
 //
 // Its working memory is a file-scope device array, reserved when the module is loaded:
 // STATIC_LANES lanes of 2^STATIC_TT_LOG2 TT buckets, their frame stacks, TT generations and
-// the counter words (41.6 MB in all). A call only enqueues work: two memsets and one launch
-// on the caller's stream; it never calls cudaMalloc, cudaFree or an allocating library.
+// the counter words (42.6 MB in all: 41.9 MB of TTs, 0.66 MB of stacks). A call only
+// enqueues work: two memsets and one launch on the caller's stream; it never calls
+// cudaMalloc, cudaFree or an allocating library. It runs the pooled solver's default
+// schedule (at most 3 cheap stages per lane per pass).
 //
 // What must start at zero: the TT tag lines and the lanes' TT generations, which static
 // device storage is when the module loads; later calls keep them (each job starts a new
@@ -29,6 +31,7 @@ constexpr size_t OFF_STACKS = round256(TT_BYTES);
 constexpr size_t OFF_GEN = OFF_STACKS + round256(STACK_BYTES);
 constexpr size_t OFF_CNT = OFF_GEN + round256(GEN_BYTES);
 constexpr size_t SCRATCH_BYTES = OFF_CNT + round256(CNT_BYTES);
+static_assert(SCRATCH_BYTES / 100000 == 426, "the scratch size stated in ddg.h is 42.6 MB");
 
 static __device__ __align__(256) unsigned char g_scratch[SCRATCH_BYTES];
 
@@ -80,6 +83,7 @@ extern "C" int ddg_solve_static(const uint64_t* d_hands, int64_t n, uint8_t* d_o
   a.tt_log2 = STATIC_TT_LOG2;
   a.free_below = 64;
   a.free_steps = 256;
+  a.cheap_limit = 3;  // the pooled solver's default schedule (ddg_config.cheap_limit = 0)
   CUDA_TRY(cudaMemsetAsync(a.counters, 0, CNT_BYTES, stream));
   CUDA_TRY(cudaMemsetAsync(d_out20, 0xFF, (size_t)n * 20, stream));
   void* params[] = {&a};

@@ -57,6 +57,7 @@ struct ProbeOut {  // a probe's answer (1, 0, or -1 = unknown), best-move hint, 
 struct TTStats {
   u64 bytes;  // tag lines and entries read + written
   u32 probes, hits, stores;
+  u32 entry_reads;  // tag-matched entries a probe read (16 bytes each)
 };
 
 DDG_HD void tags_load(const TTBucket* b, u32* t) {
@@ -138,6 +139,7 @@ DDG_CALL ProbeOut tt_probe(const TTBucket* tt, const NodeKey& k, int need, TTSta
     u64 w0, w1;
     entry_load(b, (int)((ways >> (4 * pos)) & 15), w0, w1);
     st.bytes += 16;
+    st.entry_reads++;
     if ((w0 & ((1ull << Q_BITS) - 1)) != k.q) continue;
     u64 owners = (w1 >> 16) | ((w0 >> 53) << 48);
     int off = 0;

@@ -88,6 +88,8 @@ typedef struct ddg_stats {
   double kernel_ms;        /* device time of the solve kernel (CUDA events) */
   int lanes;               /* lanes launched */
   int grid, block;         /* launch shape */
+  uint64_t tt_entry_reads; /* tag-matched entries read by probes (16 bytes each): the TT's
+                              algorithmic bytes are 64 * probes + 16 * entry reads + 80 * stores */
 } ddg_stats;
 
 const char* ddg_version(void);
@@ -110,6 +112,9 @@ uint64_t ddg_solver_nodes(const ddg_solver* s);
  * deal * jobs_per_deal + strain (jpd 5) or + strain * 4 + declarer (jpd 20)); NULL stops
  * it. No counterpart in the reference, which reports no latency (per-job tails, p99). */
 int ddg_solver_set_job_times(ddg_solver* s, uint64_t* d_job_end_ns);
+/* The same for the time each job was taken by a lane (its search time is end - start);
+ * d_job_start_ns: n * jobs_per_deal words, 0 = not started; NULL stops it. */
+int ddg_solver_set_job_starts(ddg_solver* s, uint64_t* d_job_start_ns);
 
 /* Solves n deals (hands: n*4 uint64, host memory) for all 5 strains and 4 declarers;
  * out20: n*20 bytes, host memory. Replaces the reference's batch of dd_solve_strain calls
@@ -193,8 +198,18 @@ int ddg_stream_close(ddg_stream* st, int drain, ddg_stats* st_out);
 
 /* One strain of one deal, declarers N,E,S,W (tricks as ints): the reference's
  * dd_solve_strain (src/dd.h:926) and dd_solve_strain_guess (src/dd.h:915; ns4 = NS seeds,
- * NULL = binary search). For many deals use ddg_solve_batch. */
+ * NULL = binary search). One job on the GPU with a fresh TT generation, so its node count
+ * is the reference's for the same call. For many deals use ddg_solve_batch. */
 int ddg_solve_strain(ddg_solver* s, const uint64_t* hands4, int strain, const int* ns4, int* out4);
+
+/* NS tricks of one lead: `leader` (0..3 = N,E,S,W) on lead in `strain`, with a fresh TT
+ * generation. stepping = 0: the reference's dd_ns_tricks (src/dd.h:877-891), a binary
+ * search over targets whose first target is `guess` clamped to 1..13; stepping = 1:
+ * dd_ns_tricks_from (src/dd.h:898-912), stepping up or down from `guess` clamped to
+ * 0..tricks left (a right guess costs two searches). The reference's calls read the deal
+ * and trump from the caller's DDCtx; here they are arguments. *ns_out = NS tricks. */
+int ddg_ns_tricks(ddg_solver* s, const uint64_t* hands4, int strain, int leader, int guess, int stepping,
+                  int* ns_out);
 
 /* The learned guide (no counterpart in the reference; it plugs into the reference's seams
  * for an N seed, src/dd.h:898-924, and a move hint, src/dd.h:562,594-600). An MLP of

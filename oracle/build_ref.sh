@@ -7,6 +7,10 @@ set -euo pipefail
 HERE="$(cd "$(dirname "$0")" && pwd)"
 REF_DIR="${REF_DIR:-/root/reference}"
 OUT="$HERE/_ref"
+if [ "${1:-}" = "--where" ]; then  # prints the reference tree this recipe reads
+  echo "$REF_DIR"
+  exit 0
+fi
 if [ ! -f "$REF_DIR/src/dd.h" ]; then
   echo "build_ref: $REF_DIR/src/dd.h not found; reference oracle not built" >&2
   exit 3

@@ -1,7 +1,8 @@
 """Regenerates the golden fixtures of tests/golden/ from the reference solver itself
 (oracle/_ref/libddref.so, built by oracle/build_ref.sh from the reference's headers).
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py          # all fixtures
+    python tests/golden/make_golden.py mixed    # only the uneven-hardness one
 
 Each fixture holds seeded deals (tests/golden/deals_np.py), the reference's trick tables
 (dd_solve_strain, src/dd.h:926) and its search-node count per job, with one job per
@@ -17,7 +18,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, HERE)
-from deals_np import make_deals  # noqa: E402
+from deals_np import make_deals, make_deals_mixed  # noqa: E402
 
 P = ctypes.c_void_p
 REF = ctypes.CDLL(os.path.join(ROOT, "oracle", "_ref", "libddref.so"))
@@ -67,7 +68,22 @@ def fixture(name, seed, n, k, tt_log2=10, wave20=True):
     return h, t5
 
 
+def mixed_fixture(name, seed, n, k_min=5, k_max=13, skew=0.3, tt_log2=10):
+    """Uneven-hardness deals (K ~ U{k_min..k_max}, a share `skew` with a 7-10 card suit
+    facing a void), the workload of the persistent uneven batch."""
+    h = make_deals_mixed(seed, 0, n, k_min, k_max, skew)
+    t5, n5 = ref_solve(h, tt_log2)
+    np.savez_compressed(os.path.join(HERE, name), seed=seed, k_min=k_min, k_max=k_max, skew=skew,
+                        tt_log2=tt_log2, hands=h, tricks=t5, nodes_jpd5=n5)
+    print(name, n, "deals", int(n5.sum()), "nodes")
+
+
 def main():
+    only = sys.argv[1:]
+    if only:  # regenerate the named fixtures only
+        if "mixed" in only:
+            mixed_fixture("mixed_300.npz", seed=3000, n=300)
+        return
     # Config 1: K=6 endings, 4096 deals, TT_LOG2=10.
     fixture("k6_4096.npz", seed=1, n=4096, k=6)
     # Endings of every size the brute-force oracle and the search both cover.
@@ -90,6 +106,8 @@ def main():
     np.savez_compressed(os.path.join(HERE, "k8_200_seeded.npz"), seed=400, k=8, tt_log2=10, hands=h,
                         seeds=seeds, tricks=tg, nodes_jpd5=ng)
     print("k8_200_seeded.npz", int(ng.sum()), "nodes")
+    # Uneven-hardness deals, K = 5..13, 30 % skewed.
+    mixed_fixture("mixed_300.npz", seed=3000, n=300)
 
 
 if __name__ == "__main__":

@@ -23,7 +23,7 @@ struct HostEnv {
   int* out20;
   uint64_t* job_nodes;
   std::atomic<long long>* next;
-  Frame stack[64];
+  Frame stack[STACK_DEPTH];
   TTBucket* tt;
   u32 mask;
   u64 start_nodes;
@@ -37,7 +37,8 @@ struct HostEnv {
   void task_started() { start_nodes = st.nodes; }
   u64 tt_key_ = 0;
   u64& tt_key() { return tt_key_; }
-  int root_hint(const Lane&) { return -1; }
+  const int8_t* hints = nullptr;  // n*20 root leads to try first (the guide's), or null
+  int root_hint(const Lane& L) { return hints ? (int)hints[L.deal * 20 + L.strain * 4 + L.decl] : -1; }
   int cheap_limit() { return 0; }
   bool fuse_follow() { return false; }
   void root_best(const Lane&, int) {}
@@ -189,10 +190,20 @@ int replay_block(const uint64_t* hands, long long n, int tt_log2, int jpd, int l
 
 
 // n deals, jpd 5 or 20 jobs per deal, mode 0 (binary search) / 1 (stepping from seeds).
-// stats[0..4] = nodes, probes, hits, stores, TT bytes; stats[5..11] = enter exits.
+// stats[0..4] = nodes, probes, hits, stores, TT bytes; stats[5..11] = enter exits;
+// stats[12] = accesses a bounds-checked build found out of range.
+int replay_solve_hinted(const uint64_t* hands, long long n, int tt_log2, int jpd, int mode, const int8_t* seeds,
+                        const int8_t* hints, int threads, int* out20, uint64_t* job_nodes, uint64_t* stats);
 int replay_solve(const uint64_t* hands, long long n, int tt_log2, int jpd, int mode,
                  const int8_t* seeds, int threads, int* out20, uint64_t* job_nodes,
                  uint64_t* stats) {
+  return replay_solve_hinted(hands, n, tt_log2, jpd, mode, seeds, nullptr, threads, out20, job_nodes, stats);
+}
+
+// replay_solve with the learned guide's root leads (hints: n*20, strain*4 + declarer; -1 =
+// none), as ddg_solve_device_ex's d_hint20.
+int replay_solve_hinted(const uint64_t* hands, long long n, int tt_log2, int jpd, int mode, const int8_t* seeds,
+                        const int8_t* hints, int threads, int* out20, uint64_t* job_nodes, uint64_t* stats) {
   if (tt_log2 < TT_MIN_LOG2 || tt_log2 > 22 || (jpd != 5 && jpd != 20)) return -1;
   if (threads <= 0) threads = (int)std::thread::hardware_concurrency();
   std::atomic<long long> next{0};
@@ -208,6 +219,7 @@ int replay_solve(const uint64_t* hands, long long n, int tt_log2, int jpd, int m
       env->jpd = jpd;
       env->mode = mode;
       env->seeds = seeds;
+      env->hints = hints;
       env->out20 = out20;
       env->job_nodes = job_nodes;
       env->next = &next;
@@ -223,8 +235,9 @@ int replay_solve(const uint64_t* hands, long long n, int tt_log2, int jpd, int m
     });
   for (auto& th : pool) th.join();
   if (stats) {
-    memset(stats, 0, 12 * sizeof(uint64_t));
+    memset(stats, 0, 13 * sizeof(uint64_t));
     for (auto& s : lane_stats) {
+      stats[12] += s.bounds;
       stats[0] += s.nodes;
       stats[1] += s.tt.probes;
       stats[2] += s.tt.hits;

@@ -1,6 +1,6 @@
-"""The reference arm of bench.py runs on host cores, so its JSON line can be checked here:
-one line with the keys the GPU arm prints, the CPU solver's figures in `cpu_baseline` and
-`e2e` equal to its own value (host only, no copies)."""
+"""bench.py's contract pieces that need no GPU: the reference arm's JSON line (it runs on
+host cores and loads nothing of the product), its rank handling, and what --gpus N does
+in each launch situation."""
 import json
 import os
 import subprocess
@@ -8,8 +8,11 @@ import sys
 
 from conftest import ROOT
 
+sys.path.insert(0, ROOT)
+import bench  # noqa: E402
+
 KEYS = {"metric", "value", "unit", "impl", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
-        "scaling", "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"}
+        "scaling", "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e", "parity", "nodes_per_s"}
 
 
 def run_bench(*args, env=None):
@@ -20,19 +23,46 @@ def run_bench(*args, env=None):
 
 
 def test_reference_arm_line():
-    lines = run_bench("--impl", "reference", "--steps", "1", "--warmup", "3", "--slice-s", "0.5")
+    lines = run_bench("--impl", "reference", "--steps", "2", "--warmup", "2", "--slice-s", "1")
     assert len(lines) == 1
     d = json.loads(lines[0])
     assert KEYS <= set(d)
     assert d["impl"] == "reference" and d["unit"] == "deals/s" and d["higher_is_better"] is True
-    assert d["steps"] == 1 and d["warmup"] == 3 and d["n_gpus"] == 1 and d["scaling"] == "weak"
-    assert d["config"]["workload"] and d["config"]["jobs_per_deal"] == 5
+    assert d["steps"] == 2 and d["warmup"] == 2 and d["n_gpus"] == 1 and d["scaling"] == "weak"
+    assert d["config"] == bench.config_dict(bench.parse(["--slice-s", "1"]), 1)  # the GPU arm's config
     cpu = d["cpu_baseline"]
     assert cpu["kind"] in ("reference", "port") and cpu["cores"] >= 1 and cpu["value"] == d["value"] > 0
     assert d["e2e"] == {"value": d["value"], "unit": "deals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    # value = the CPU's node rate over the workload's mean nodes per deal
+    assert abs(d["value"] - d["nodes_per_s"] / d["nodes_per_deal"]["nodes_per_deal"]) < 1e-9 * d["value"]
+    assert d["parity"]["equal"] is True and d["parity"]["checked"] > 0
+
+
+def test_reference_arm_loads_nothing_of_the_product():
+    code = ("import sys, json; sys.argv = ['bench.py', '--impl', 'reference', '--steps', '1', '--warmup', '1', "
+            "'--slice-s', '0.5']; import bench; bench.main(sys.argv[1:]); "
+            "maps = open('/proc/self/maps').read(); print(json.dumps({'ddg': 'libddg' in maps}))")
+    r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert json.loads(r.stdout.strip().splitlines()[-1]) == {"ddg": False}
 
 
 def test_reference_arm_other_ranks_print_nothing():
     env = dict(os.environ, RANK="1", LOCAL_RANK="1", WORLD_SIZE="2")
     assert run_bench("--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "3", "--slice-s", "0.5",
                      env=env) == []
+
+
+def test_gpus_launch_plan():
+    assert bench.launch_plan(1, {}) == "run"
+    assert bench.launch_plan(4, {}) == "spawn"            # starts its own 4 ranks
+    assert bench.launch_plan(4, {"WORLD_SIZE": "4"}) == "run"
+    assert bench.launch_plan(8, {"WORLD_SIZE": "2"}) == "refuse"
+    assert bench.launch_plan(1, {"WORLD_SIZE": "1"}) == "run"
+
+
+def test_gpus_mismatch_is_refused():
+    env = dict(os.environ, RANK="0", LOCAL_RANK="0", WORLD_SIZE="2")
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--gpus", "4"], cwd=ROOT,
+                       capture_output=True, text=True, timeout=120, env=env)
+    assert r.returncode == 2 and "--gpus 4" in r.stderr

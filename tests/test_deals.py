@@ -11,6 +11,15 @@ def test_generator_matches_restatement(ddg):
         assert (a == b).all()
 
 
+def test_mixed_generator_matches_restatement(ddg):
+    from deals_np import make_deals_mixed
+    for seed, first, n, kmin, kmax, skew in ((3000, 0, 300, 5, 13, 0.3), (7, 500, 100, 7, 10, 0.6),
+                                             (1, 0, 50, 13, 13, 1.0)):
+        a = ddg.make_deals_mixed(seed, first, n, kmin, kmax, skew)
+        b = make_deals_mixed(seed, first, n, kmin, kmax, skew)
+        assert (a == b).all()
+
+
 def test_generator_random_access(ddg):
     whole = ddg.make_deals(7, 0, 50, 13)
     part = ddg.make_deals(7, 20, 10, 13)

@@ -50,7 +50,10 @@ def test_two_ranks_shard_and_combine():
         p.join(timeout=60)
         assert p.exitcode == 0
     (h0, s0, o0), (h1, s1, o1) = res[0], res[1]
-    assert s0 == s1 == (20000, 4)               # same work per rank (weak scaling)
+    import sys
+    sys.path.insert(0, ROOT)
+    import bench
+    assert s0 == s1 == (bench.SET_SIZE, 4)      # same work per rank (weak scaling)
     assert not (h0 == h1).all(axis=1).any()     # different deals
     assert o0 == o1                             # every rank gets the same combined figures
     elapsed, e2e, jobs, e2e_jobs, nodes = o0

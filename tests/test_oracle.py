@@ -15,7 +15,10 @@ from deals_np import make_deals
 P = ctypes.c_void_p
 ORACLE_DIR = os.path.join(ROOT, "oracle")
 REF_SO = os.path.join(ORACLE_DIR, "_ref", "libddref.so")
-PGX = "/root/reference/data/deals_20k.npy"
+# The reference tree, as the recipe that compiles it resolves it (REF_DIR or its default).
+REF_DIR = subprocess.run(["bash", os.path.join(ORACLE_DIR, "build_ref.sh"), "--where"], capture_output=True,
+                         text=True).stdout.strip()
+PGX = os.path.join(REF_DIR, "data", "deals_20k.npy")
 
 
 @pytest.fixture(scope="session")
