@@ -427,7 +427,7 @@ def our_arm(a, rank, world, local_rank):
                         "nodes_per_s": nps, "nodes_per_deal": cost,
                         "finished_deals_per_s": jobs_all / JPD / (ms * 1e-3), "jobs_finished": int(jobs_all),
                         "nodes_per_s_by_step": [st["nodes"] / (st["kernel_ms"] * 1e-3) for st in run["stats"]],
-                        "job_ms": run["lat"], "lanes_idle": not run["started_all"], "ms": ms}
+                        "job_ms": run["lat"], "queue_ran_dry": run["started_all"], "ms": ms}
     e2e_ms_all, _, e2e_nodes_all, _, _ = combine_ranks(world, dev, e2e_ms or 0.0, None, e2e_nodes, 0, 0)
 
     cpu = cpu_tables = None

@@ -84,21 +84,30 @@ DDG_HD void tags_store(TTBucket* b, const u32* t) {
   for (int k = 0; k < TT_WAYS; k++) b->tag[k] = t[k];
 #endif
 }
+// An entry's first word is stored sealed with its second: e0 = w0 ^ seal(w1). A reader
+// unseals with the w1 it read, so a torn entry (words of two different stores, which
+// lanes sharing one TT can produce) decodes to a garbled q and fails the probe's key
+// check instead of pairing one position's bounds with another's pattern. An untorn entry
+// decodes exactly, so every decision, and every node count, is unchanged.
+DDG_HD u64 seal(u64 w1) {
+  u64 x = (w1 ^ (w1 >> 29)) * 0xBF58476D1CE4E5B9ull;
+  return x ^ (x >> 32);
+}
 DDG_HD void entry_load(const TTBucket* b, int way, u64& w0, u64& w1) {
 #ifdef __CUDA_ARCH__
   ulonglong2 x = *reinterpret_cast<const ulonglong2*>(b->e[way]);
-  w0 = x.x;
   w1 = x.y;
+  w0 = x.x ^ seal(x.y);
 #else
-  w0 = b->e[way][0];
   w1 = b->e[way][1];
+  w0 = b->e[way][0] ^ seal(w1);
 #endif
 }
 DDG_HD void entry_store(TTBucket* b, int way, u64 w0, u64 w1) {
 #ifdef __CUDA_ARCH__
-  *reinterpret_cast<ulonglong2*>(b->e[way]) = make_ulonglong2(w0, w1);
+  *reinterpret_cast<ulonglong2*>(b->e[way]) = make_ulonglong2(w0 ^ seal(w1), w1);
 #else
-  b->e[way][0] = w0;
+  b->e[way][0] = w0 ^ seal(w1);
   b->e[way][1] = w1;
 #endif
 }
@@ -226,9 +235,9 @@ DDG_CALL void tt_store(TTBucket* tt, const NodeKey& k, u32 gen, u64 rel, int lb,
       if (oub < ub) ub = oub;
       if (best < 0 && obest != 63) best = obest;
 #ifdef __CUDA_ARCH__
-      reinterpret_cast<u64*>(b->e[way])[0] = pack_w0(k, lb, ub, best, hi);
+      reinterpret_cast<u64*>(b->e[way])[0] = pack_w0(k, lb, ub, best, hi) ^ seal(e1);
 #else
-      b->e[way][0] = pack_w0(k, lb, ub, best, hi);
+      b->e[way][0] = pack_w0(k, lb, ub, best, hi) ^ seal(e1);
 #endif
       st.bytes += 8;
       return;
