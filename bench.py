@@ -55,8 +55,10 @@ JPD = 5
 SAMPLE = os.path.join(ROOT, "tests", "golden", "k13_bench_2000.npz")
 GUIDED_SAMPLE = os.path.join(ROOT, "tests", "golden", "k13_bench_2000_guided.npz")
 # DRAM bytes (read + write) per search node of one launch of this workload's own shape
-# (TT 2^10, full grid, steady state), from `bench.py --profile-case` under ncu.
-DRAM_BYTES_PER_NODE = None
+# (TT 2^10, 75,776 lanes, third 0.5 s slice), from `bench.py --profile-case --warmup 2
+# --slice-s 0.5` under ncu (dram__bytes_read.sum + dram__bytes_write.sum = 27.04 + 10.04
+# GB over 350.2 M nodes).
+DRAM_BYTES_PER_NODE = 105.9
 WORKLOAD = ("13-card seeded random deals, all 5 strains x 4 declarers, exact TT 2^10 buckets per lane, "
             "one job per (deal, strain)")
 

@@ -62,6 +62,7 @@ struct ddg_solver {
   uint64_t* d_job_start_ns = nullptr;  // caller's buffer for the times jobs were taken, or null
   uint64_t start_ns = 0;             // device global timer at the last solve's launch
   TaskPool* tasks = nullptr;         // helping's task pool (cfg.help), cleared per solve
+  size_t tasks_bytes = 0;            // the pool and, after it, one TT-user count per lane
   // Resumable (time-sliced) solve.
   LaneSave* save = nullptr;  // lanes x LaneSave, allocated by the first ddg_solve_begin
   BatchArgs slice_args;
@@ -245,7 +246,8 @@ int ddg_solver_create(const ddg_config* cfg_in, ddg_solver** out) {
   if (e == cudaSuccess) e = cudaMalloc(&s->stacks, st_bytes);
   if (e == cudaSuccess) e = cudaMalloc(&s->lane_gen, (size_t)lanes * 4);
   if (e == cudaSuccess) e = cudaMalloc(&s->counters, CNT_WORDS * 8);
-  if (e == cudaSuccess && cfg.help) e = cudaMalloc(&s->tasks, sizeof(TaskPool));
+  s->tasks_bytes = (sizeof(TaskPool) + 255) / 256 * 256 + (size_t)lanes * sizeof(int);
+  if (e == cudaSuccess && cfg.help) e = cudaMalloc(&s->tasks, s->tasks_bytes);
   if (e == cudaSuccess) e = cudaMemset(s->tt, 0, tt_bytes);
   if (e == cudaSuccess) e = cudaMemset(s->lane_gen, 0, (size_t)lanes * 4);
   if (e == cudaSuccess) e = cudaHostAlloc(&s->h_stop, sizeof(int), cudaHostAllocMapped);
@@ -319,6 +321,9 @@ static BatchArgs make_args(ddg_solver* s, const uint64_t* d_hands, int64_t n, co
   a.job_end_ns = s->d_job_end_ns;
   a.job_start_ns = s->d_job_start_ns;
   a.tasks = s->tasks;
+  a.share_tt = s->tasks && s->cfg.help_share_tt;
+  a.tt_users = s->tasks ? reinterpret_cast<int*>(reinterpret_cast<char*>(s->tasks) + (sizeof(TaskPool) + 255) / 256 * 256)
+                        : nullptr;
   a.free_below = s->cfg.free_below == 0 ? 64 : s->cfg.free_below < 0 ? 0 : s->cfg.free_below;
   a.free_steps = s->cfg.free_steps > 0 ? s->cfg.free_steps : 256;
   a.next_job = s->counters + CNT_NEXT_JOB;
@@ -411,7 +416,7 @@ int ddg_solve_device_ex(ddg_solver* s, const uint64_t* d_hands, int64_t n, const
   CUDA_TRY(cudaMemsetAsync(d_out20, 0xFF, (size_t)n * 20, stream));
   if (d_best20) CUDA_TRY(cudaMemsetAsync(d_best20, 0xFF, (size_t)n * 20, stream));
   *(volatile int*)s->h_stop = 0;
-  if (s->tasks) CUDA_TRY(cudaMemsetAsync(s->tasks, 0, sizeof(TaskPool), stream));
+  if (s->tasks) CUDA_TRY(cudaMemsetAsync(s->tasks, 0, s->tasks_bytes, stream));
   if (s->d_job_end_ns) CUDA_TRY(cudaMemsetAsync(s->d_job_end_ns, 0, (size_t)a.n_jobs * 8, stream));
   if (s->d_job_start_ns) CUDA_TRY(cudaMemsetAsync(s->d_job_start_ns, 0, (size_t)a.n_jobs * 8, stream));
   CUDA_TRY(cudaEventRecord(s->ev0, stream));
@@ -452,7 +457,7 @@ int ddg_solve_graph(ddg_solver* s, const uint64_t* d_hands, int64_t n, const int
     cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) e = cudaMemsetAsync(s->counters, 0, CNT_WORDS * 8, cap);
     if (e == cudaSuccess) e = cudaMemsetAsync(d_out20, 0xFF, (size_t)n * 20, cap);
-    if (e == cudaSuccess && s->tasks) e = cudaMemsetAsync(s->tasks, 0, sizeof(TaskPool), cap);
+    if (e == cudaSuccess && s->tasks) e = cudaMemsetAsync(s->tasks, 0, s->tasks_bytes, cap);
     if (e == cudaSuccess && s->d_job_end_ns) e = cudaMemsetAsync(s->d_job_end_ns, 0, (size_t)a.n_jobs * 8, cap);
     if (e == cudaSuccess && s->d_job_start_ns)
       e = cudaMemsetAsync(s->d_job_start_ns, 0, (size_t)a.n_jobs * 8, cap);
@@ -514,7 +519,7 @@ int ddg_solve_begin_ex(ddg_solver* s, const uint64_t* d_hands, int64_t n, const 
   s->slice_n = n;
   CUDA_TRY(cudaMemsetAsync(s->counters, 0, CNT_WORDS * 8, stream));
   CUDA_TRY(cudaMemsetAsync(d_out20, 0xFF, (size_t)n * 20, stream));
-  if (s->tasks) CUDA_TRY(cudaMemsetAsync(s->tasks, 0, sizeof(TaskPool), stream));
+  if (s->tasks) CUDA_TRY(cudaMemsetAsync(s->tasks, 0, s->tasks_bytes, stream));
   if (s->d_job_end_ns) CUDA_TRY(cudaMemsetAsync(s->d_job_end_ns, 0, (size_t)s->slice_args.n_jobs * 8, stream));
   if (s->d_job_start_ns)
     CUDA_TRY(cudaMemsetAsync(s->d_job_start_ns, 0, (size_t)s->slice_args.n_jobs * 8, stream));
@@ -878,7 +883,7 @@ static int solve_one(ddg_solver* s, const uint64_t* hands4, int strain, int decl
   a.first_target = first_target;
   CUDA_TRY(cudaMemset(s->counters, 0, CNT_WORDS * 8));
   CUDA_TRY(cudaMemset(s->d_out, 0xFF, 20));
-  if (s->tasks) CUDA_TRY(cudaMemset(s->tasks, 0, sizeof(TaskPool)));
+  if (s->tasks) CUDA_TRY(cudaMemset(s->tasks, 0, s->tasks_bytes));
   *(volatile int*)s->h_stop = 0;
   CUDA_TRY(cudaEventRecord(s->ev0, nullptr));
   int grid = 0;

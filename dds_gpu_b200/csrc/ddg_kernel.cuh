@@ -57,6 +57,8 @@ struct BatchArgs {
   u64* job_end_ns;       // n * jpd completion times (device global timer, ns), or null
   u64* job_start_ns;     // n * jpd times the jobs were taken by a lane, or null
   TaskPool* tasks;       // helping: idle lanes take donated moves (tricks exact), or null
+  int share_tt;          // helping: a helper searches in its donor's TT (else in its own)
+  int* tt_users;         // helping with shared TTs: per lane, helpers searching in its TT
   int free_below;        // fewer busy lanes than this in a block: each thread runs its own lane
   int free_steps;        // stages a lane runs per free-running round
   struct LaneSave* save; // resumable solve: lane states kept between launches, or null
@@ -132,6 +134,7 @@ __device__ __forceinline__ void lane_begin(const BatchArgs& a, long long lane, L
   L.r = 0;
   L.p.trick = 0;
   L.task = -1;
+  L.owner = -1;
 }
 
 // End of a launch: the TT generation, and for a resumable solve the lane's state.
@@ -163,6 +166,14 @@ struct DevEnv {
 
   __device__ __forceinline__ LaneStats& stats() { return c->s; }
   __device__ __forceinline__ TaskPool* pool() { return tp; }
+  __device__ __forceinline__ TTBucket* tt_of(int owner) const { return a->tt + ((long long)owner << a->tt_log2); }
+  __device__ __forceinline__ long long self() const { return lane; }
+  __device__ __forceinline__ bool share_tt() const { return a->share_tt != 0; }
+  __device__ __forceinline__ void tt_users_add(int owner, int d) { atomicAdd(a->tt_users + owner, d); }
+  __device__ __forceinline__ int tt_users(int owner) {
+    __threadfence();  // the job's last task operations before the count is read
+    return atom_load(a->tt_users + owner);
+  }
   __device__ __forceinline__ bool want_donation() {
     if (!*help_hint) return false;
     const int q = atomicAdd(&tp->queued, 1);

@@ -397,6 +397,8 @@ struct Task {
   int8_t v;         // result: value of the donated part
   int8_t best;      // result: the cutting card, or -1
   u64 key;          // (deal << 3 | strain) + 1 of the donor: helpers keep their TT per key
+  int32_t owner;    // the lane whose TT the donor's search uses (shared-TT helping)
+  u32 gen;          // that TT's generation for the donor's job
 };
 
 // The tasks of a launch and the counters that steer helping (HBM on the GPU).
@@ -556,7 +558,9 @@ struct Lane {
   Top top;    // trick-start table of an expanding lead node (ENTER -> MOVES_LEAD)
   u64 r;    // relevant cards of the node just finished
   long long job, deal;
-  u32 gen;
+  u32 gen;           // generation of the lane's own TT
+  int32_t owner;     // shared-TT helping: the lane whose TT this task's search uses, -1 = own
+  u32 hgen;          // and that TT's generation for the donor's job
   int16_t task;      // the task this lane helps with, or -1 (its own job)
   int8_t par_sp;     // depth of `par`, or -1
   int8_t stage, sp;  // sp = depth of f; frames 0..sp-1 are in the lane's stack
@@ -565,6 +569,16 @@ struct Lane {
   int8_t mode, decl, last_decl, strain;
   int8_t v;  // value of the node just finished
 };
+
+// The TT a lane's search reads and writes, and its generation: the lane's own, or, for a
+// helper with shared-TT helping, the donor's (entries are facts about positions of one
+// deal and trump, so every lane searching parts of one job may share them; a helper's
+// findings then serve the donor and the other helpers of the job, and theirs serve it).
+template <class Env>
+DDG_HD TTBucket* search_tt(const Lane& L, Env& env) {
+  return L.owner >= 0 ? env.tt_of(L.owner) : env.tt;
+}
+DDG_HD u32 search_gen(const Lane& L) { return L.owner >= 0 ? L.hgen : L.gen; }
 
 // Sets up the search of declarer `decl`'s lead (leader = decl + 1) at `target`.
 DDG_HD void start_search(Lane& L) {
@@ -714,6 +728,13 @@ DDG_CALL void node_done(Lane& L, Env& env) {
 template <class Env>
 DDG_CALL void step_take(Lane& L, Env& env) {
   TaskPool* tp = env.pool();
+  // Shared-TT helping: helpers still writing into this lane's TT (an abandoned task that
+  // has not yet seen it is abandoned) hold the TT for the finished job; the next job, with
+  // its new generation and possibly a tag clear, waits for them.
+  if (tp && env.share_tt() && env.tt_users(env.self()) > 0) {
+    L.stage = ST_TAKE;
+    return;
+  }
   const int got = env.take(L);
   if (got < 0) {  // a stream with no deal published yet: try again later
     L.stage = ST_TAKE;
@@ -731,6 +752,7 @@ DDG_CALL void step_take(Lane& L, Env& env) {
   }
   if (tp) atom_add(&tp->busy, 1);
   L.task = -1;
+  L.owner = -1;
   L.p.trump = strain_trump(L.strain);
   L.p.trick = 0;
   L.gen = tt_next_gen(env.tt, env.mask, L.gen);
@@ -766,7 +788,8 @@ DDG_CALL void step_root(Lane& L, Env& env) {
 template <class Env>
 DDG_HD void step_enter(Lane& L, Env& env) {
   const bool lead = L.p.nplayed == 0;
-  int e = lead ? enter_lead(L.p, L.target, L.f, L.r, L.top, env.tt, env.mask, L.gen, env.stats())
+  int e = lead ? enter_lead(L.p, L.target, L.f, L.r, L.top, search_tt(L, env), env.mask, search_gen(L),
+                            env.stats())
                : enter_follow(L.p, L.target, L.f, L.r, env.stats());
   if (e < 0) {
     L.stage = lead ? ST_MOVES_LEAD : ST_MOVES_FOLLOW;
@@ -807,12 +830,16 @@ DDG_CALL void frame_done(Lane& L, Env& env) {
     TaskPool& tp = *env.pool();
     task_finish(tp, L.task, L.v, f.acc, fr_best(f));
     L.task = -1;
+    if (L.owner >= 0) {  // done with the donor's TT
+      env.tt_users_add(L.owner, -1);
+      L.owner = -1;
+    }
     atom_add(&tp.busy, -1);
     atom_add(&tp.hungry, 1);
     L.stage = ST_HUNGRY;
     return;
   }
-  L.r = finish(L.p, f, env.tt, env.mask, L.gen, env.stats());
+  L.r = finish(L.p, f, search_tt(L, env), env.mask, search_gen(L), env.stats());
   node_done(L, env);
 }
 
@@ -845,7 +872,7 @@ DDG_CALL void step_next(Lane& L, Env& env) {
       L.par_sp = L.sp;
       L.sp++;
       if (L.p.nplayed == 0)  // a trick start next: its TT tag line, on its way to L2
-        prefetch_l2(env.tt + (key_hash(length_key(L.p.h), L.p.leader) & env.mask));
+        prefetch_l2(search_tt(L, env) + (key_hash(length_key(L.p.h), L.p.leader) & env.mask));
       L.stage = ST_ENTER;
       return;
     }
@@ -951,6 +978,20 @@ DDG_CALL bool step_hungry(Lane& L, Env& env) {
   L.task = (int16_t)t;
   L.deal = (long long)((k.key - 1) >> 3);
   L.strain = (int8_t)((k.key - 1) & 7);
+  L.stage = ST_NEXT;
+  if (env.share_tt()) {
+    // The helper searches in the donor's TT. It registers as a user of that TT first and
+    // then checks that the task is still running: a donor abandons a task before it can
+    // finish its job, and looks at its TT's users only after that, so either it sees this
+    // helper registered, or the helper sees the task abandoned and stops before touching
+    // the TT.
+    env.tt_users_add(k.owner, 1);
+    L.owner = k.owner;
+    L.hgen = k.gen;
+    fence_block();
+    if (atom_load(&tp.state[t]) == TASK_ABANDONED) abort_task(L, env);
+    return true;
+  }
   // Entries of the TT are facts about positions of one deal and trump suit: a helper that
   // stays on the same (deal, strain) keeps them, which spares it re-searching the subtrees
   // its earlier tasks already solved.
@@ -958,7 +999,6 @@ DDG_CALL bool step_hungry(Lane& L, Env& env) {
     L.gen = tt_next_gen(env.tt, env.mask, L.gen);
     env.tt_key() = k.key;
   }
-  L.stage = ST_NEXT;
   return true;
 }
 
@@ -980,6 +1020,11 @@ DDG_CALL void abort_task(Lane& L, Env& env) {
   const bool top_is_own = L.stage == ST_NEXT || L.stage == ST_RET || L.stage == ST_WAIT;
   if (top_is_own && fr_task(L.f) >= 0 && DDG_IN_BOUNDS(fr_task(L.f) < MAX_TASKS, env.stats()))
     task_abandon(tp, fr_task(L.f));
+  if (L.owner >= 0) {  // no more writes into the donor's TT
+    fence_block();
+    env.tt_users_add(L.owner, -1);
+    L.owner = -1;
+  }
   tp.state[L.task] = TASK_FREE;
   L.task = -1;
   atom_add(&tp.busy, -1);
@@ -1025,6 +1070,8 @@ DDG_CALL bool try_donate(Lane& L, Env& env) {
     t.info = g.info;
     t.target = L.target;
     t.key = ((u64)L.deal << 3 | (u64)L.strain) + 1;
+    t.owner = L.owner >= 0 ? L.owner : (int32_t)env.self();  // a helper passes its donor's TT on
+    t.gen = search_gen(L);
     t.r = 0;
     t.v = 0;
     t.best = -1;

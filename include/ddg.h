@@ -64,6 +64,8 @@ typedef struct ddg_config {
                            one pass of the block-phase kernel: a lane with a long chain of
                            returns no longer holds up the block's other phases; 0 = 3, -1 =
                            no limit */
+  int help_share_tt;    /* with help: 1 = a helper searches its task in the donor's TT (all
+                           lanes on parts of one job share what they learn), 0 = in its own */
 } ddg_config;
 
 /* Counters of one solve call (device-side counters, summed over lanes). */

@@ -37,6 +37,12 @@ struct HostEnv {
   void task_started() { start_nodes = st.nodes; }
   u64 tt_key_ = 0;
   u64& tt_key() { return tt_key_; }
+  // Shared-TT helping (SimEnv overrides these; a lone lane has no helpers).
+  bool share_tt() { return false; }
+  TTBucket* tt_of(int) { return tt; }
+  long long self() { return 0; }
+  void tt_users_add(int, int) {}
+  int tt_users(int) { return 0; }
   const int8_t* hints = nullptr;  // n*20 root leads to try first (the guide's), or null
   int root_hint(const Lane& L) { return hints ? (int)hints[L.deal * 20 + L.strain * 4 + L.decl] : -1; }
   int cheap_limit() { return 0; }
@@ -75,11 +81,19 @@ struct SimShared {
   int budget = 0;  // donations allowed this iteration
   bool eager = false;
   int cheap_limit = 0;  // most cheap stages per lane per pass, as the GPU kernel's
+  bool share = false;   // helpers search in their donor's TT
+  std::vector<TTBucket*> tts;  // every lane's TT
+  std::vector<int> users;      // helpers searching in each lane's TT
 };
 struct SimEnv : HostEnv {
   SimShared* sh;
   int lane_id = 0, min_nodes = 0;
   TaskPool* pool() { return &sh->pool; }
+  bool share_tt() { return sh->share; }
+  TTBucket* tt_of(int lane) { return sh->tts[lane]; }
+  long long self() { return lane_id; }
+  void tt_users_add(int lane, int d) { sh->users[lane] += d; }
+  int tt_users(int lane) { return sh->users[lane]; }
   bool want_donation() {
     if (sh->budget <= 0 || (!sh->eager && sh->pool.queued >= sh->pool.hungry)) return false;
     sh->budget--;
@@ -96,12 +110,20 @@ struct SimEnv : HostEnv {
 extern "C" {
 // n deals on one simulated block of `lanes` lanes, with helping; `eager` donates whenever a
 // lane could (not only when lanes are hungry). Results and nodes as replay_solve; stats[12]
-// = tasks posted, stats[13] = block iterations.
+// = tasks posted, stats[13] = block iterations. `share`: helpers search in their donor's TT.
+int replay_block_ex(const uint64_t* hands, long long n, int tt_log2, int jpd, int lanes, int eager, int free_below,
+                    int free_steps, int* out20, uint64_t* stats, int cheap_limit, int share);
 int replay_block(const uint64_t* hands, long long n, int tt_log2, int jpd, int lanes, int eager, int free_below,
                  int free_steps, int* out20, uint64_t* stats, int cheap_limit) {
+  return replay_block_ex(hands, n, tt_log2, jpd, lanes, eager, free_below, free_steps, out20, stats, cheap_limit, 0);
+}
+int replay_block_ex(const uint64_t* hands, long long n, int tt_log2, int jpd, int lanes, int eager, int free_below,
+                    int free_steps, int* out20, uint64_t* stats, int cheap_limit, int share) {
   if (tt_log2 < TT_MIN_LOG2 || tt_log2 > 16 || (jpd != 5 && jpd != 20) || lanes < 1 || lanes > 1024) return -1;
   std::atomic<long long> next{0};
   SimShared* sh = new SimShared();
+  sh->share = share != 0;
+  sh->users.assign(lanes, 0);
   memset(&sh->pool, 0, sizeof(sh->pool));
   std::vector<SimEnv*> envs(lanes);
   std::vector<std::vector<TTBucket>> tts(lanes);
@@ -119,6 +141,7 @@ int replay_block(const uint64_t* hands, long long n, int tt_log2, int jpd, int l
     e->job_nodes = nullptr;
     e->next = &next;
     e->tt = tts[i].data();
+    sh->tts.push_back(tts[i].data());
     e->mask = (1u << tt_log2) - 1;
     memset(&e->st, 0, sizeof(e->st));
     e->sh = sh;
@@ -128,6 +151,7 @@ int replay_block(const uint64_t* hands, long long n, int tt_log2, int jpd, int l
     memset(&L[i], 0, sizeof(Lane));
     L[i].stage = ST_TAKE;
     L[i].task = -1;
+    L[i].owner = -1;
   }
   sh->eager = eager != 0;
   sh->cheap_limit = cheap_limit;
@@ -171,6 +195,8 @@ int replay_block(const uint64_t* hands, long long n, int tt_log2, int jpd, int l
   for (int k = 0; k < MAX_TASKS; k++)
     if (sh->pool.state[k] != TASK_FREE) return -3;  // every task must be back in the pool
   if (sh->pool.busy || sh->pool.hungry || sh->pool.queued) return -4;  // and every count at zero
+  for (int u : sh->users)
+    if (u) return -5;  // every helper let go of its donor's TT
   if (stats) {
     memset(stats, 0, 14 * sizeof(uint64_t));
     for (auto* e : envs) {
@@ -229,6 +255,7 @@ int replay_solve_hinted(const uint64_t* hands, long long n, int tt_log2, int jpd
       Lane L;
       memset(&L, 0, sizeof(L));
       L.stage = ST_TAKE;
+      L.owner = -1;
       while (L.stage != ST_IDLE) lane_step(L, *env);
       lane_stats[t] = env->st;
       delete env;

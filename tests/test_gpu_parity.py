@@ -142,6 +142,24 @@ def test_helping_exact_tricks(ddg, helper_solver, name):
     assert st["jobs_done"] == g["hands"].shape[0] * 20
 
 
+@pytest.mark.parametrize("name", ["k7_120.npz", "k9_120.npz", "k6_4096.npz"])
+def test_shared_tt_helping_exact_tricks(ddg, name):
+    """Helpers search their tasks in the donor's TT, which the donor and every helper of the
+    job read and write at once (sealed entries make a torn entry a miss): tricks exact."""
+    g = load_golden(name)
+    s = ddg.Solver(tt_log2=10, jobs_per_deal=20, lanes=1024, block=256, min_blocks=2, help=1, help_share_tt=1,
+                   time_limit_s=120)
+    try:
+        t, _, st = device_solve(ddg, s, g["hands"])
+        assert (t == g["tricks"]).all()
+        assert st["jobs_done"] == g["hands"].shape[0] * 20
+        hard = load_golden("k13_24.npz")
+        t, _, st = device_solve(ddg, s, np.ascontiguousarray(hard["hands"][LIGHT_13]))
+        assert (t == hard["tricks"][LIGHT_13]).all() and st["tasks"] > 0
+    finally:
+        s.close()
+
+
 def test_helping_splits_hard_deals(ddg, helper_solver):
     """Few full deals on many lanes: lanes go hungry at once and take donated moves."""
     g = load_golden("k13_24.npz")

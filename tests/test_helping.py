@@ -51,3 +51,34 @@ def test_helping_with_cheap_limit(replay_lib, name, cheap_limit, lanes, eager, j
     rc, t, st = block(replay_lib, g["hands"][:48], lanes, eager, jpd, cheap_limit=cheap_limit)
     assert rc == 0
     assert (t == g["tricks"][:48]).all()
+
+
+def block_shared(lib, hands, lanes, eager, jpd=5, cheap_limit=0, free_below=0):
+    n = hands.shape[0]
+    h = np.ascontiguousarray(hands, dtype=np.uint64)
+    out = np.zeros(n * 20, np.int32)
+    st = np.zeros(14, np.uint64)
+    rc = lib.replay_block_ex(h.ctypes.data_as(P), ctypes.c_longlong(n), 10, jpd, lanes, eager, free_below, 17,
+                             out.ctypes.data_as(P), st.ctypes.data_as(P), cheap_limit, 1)
+    return rc, out.reshape(n, 5, 4), st
+
+
+@pytest.mark.parametrize("name", ["k5_120.npz", "k8_120.npz", "k9_120.npz"])
+@pytest.mark.parametrize("lanes,eager,jpd,cheap_limit,free", [(16, 1, 20, 0, 0), (64, 1, 5, 3, 0), (32, 0, 20, 2, 8),
+                                                              (3, 1, 5, 0, 1000)])
+def test_shared_tt_helping_keeps_tricks(replay_lib, name, lanes, eager, jpd, cheap_limit, free):
+    """Helpers search in their donor's TT: tricks stay the reference's, and every helper
+    lets go of the donor's TT (the simulator returns -5 otherwise)."""
+    g = load_golden(name)
+    rc, t, st = block_shared(replay_lib, g["hands"][:48], lanes, eager, jpd, cheap_limit, free)
+    assert rc == 0
+    assert (t == g["tricks"][:48]).all()
+    if eager:
+        assert st[12] > 0
+
+
+def test_shared_tt_helping_full_deals(replay_lib):
+    g = load_golden("k13_24.npz")
+    idx = [1, 3, 15]
+    rc, t, st = block_shared(replay_lib, g["hands"][idx], 32, 1, 20, 3)
+    assert rc == 0 and (t == g["tricks"][idx]).all() and st[12] > 0
