@@ -321,7 +321,7 @@ static BatchArgs make_args(ddg_solver* s, const uint64_t* d_hands, int64_t n, co
   a.job_end_ns = s->d_job_end_ns;
   a.job_start_ns = s->d_job_start_ns;
   a.tasks = s->tasks;
-  a.share_tt = s->tasks && s->cfg.help_share_tt;
+  a.share_tt = s->tasks && s->cfg.help_share_tt >= 0;  // 0 = the default: shared
   a.tt_users = s->tasks ? reinterpret_cast<int*>(reinterpret_cast<char*>(s->tasks) + (sizeof(TaskPool) + 255) / 256 * 256)
                         : nullptr;
   a.free_below = s->cfg.free_below == 0 ? 64 : s->cfg.free_below < 0 ? 0 : s->cfg.free_below;

@@ -263,7 +263,7 @@ struct DevEnv {
     return (long long)*reinterpret_cast<volatile unsigned long long*>(a->next_job) < avail;
   }
   __device__ __forceinline__ int seed(const Lane& L) {
-    if (a->mode == MODE_STEP) return (int)a->seeds[L.deal * 20 + L.strain * 4 + L.decl];
+    if (a->mode == MODE_STEP) return (int)a->seeds[out_row(L) * 20 + L.strain * 4 + L.decl];
     return a->first_target ? a->first_target : 7;
   }
   __device__ __forceinline__ long long out_row(const Lane& L) const {
@@ -311,6 +311,7 @@ struct BlockShared {
   LaneCounters cnt[BLOCK];
   BatchArgs args;
   unsigned mask[BLOCK / 32];
+  unsigned mask2[BLOCK / 32];  // free-running rounds: lanes waiting for a job or a task
   unsigned long long ph_warps[PH_COUNT], ph_items[PH_COUNT], iters;
   int stop;
   int help_hint;    // hungry lanes outnumber queued tasks (read once per iteration)
@@ -493,17 +494,46 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(BatchArgs a) {
       if (sh.idle_exit && st0 == ST_TAKE) sh.lane[tid].stage = ST_IDLE;
     }
     if (busy_here < a.free_below) {
-      // Few busy lanes: each thread runs its own lane for a while, no phases.
+      // Few busy lanes: each lane runs on a thread of its own for a while, no phases. The
+      // lanes with search work go first, one to a warp (the k-th to warp k mod 16, the
+      // (k div 16)-th thread of it), so up to one lane per warp runs at a lone lane's speed
+      // instead of sharing a warp's issue with the divergent paths of its neighbours;
+      // lanes waiting for a job or a task come after them.
       const long long f0 = clock64();
-      Lane& L = sh.lane[tid];
-      if (L.stage == ST_HUNGRY && sh.all_done) {
-        atomicAdd(&a.tasks->hungry, -1);
-        L.stage = ST_IDLE;
-      } else if (L.stage != ST_IDLE) {
-        DevEnv env = lane_env(sh, base + tid, tid);
-        if (env.tp && task_abandoned(L, env.tp)) abort_task(L, env);
-        const bool may_claim = L.stage == ST_HUNGRY && atomicSub(&sh.claim_slots, 1) > 0;
-        advance_free(L, env, a.free_steps, may_claim);
+      {
+        const int wid = tid >> 5, ln = tid & 31;
+        const int stg = sh.lane[tid].stage;
+        const bool work = stg != ST_IDLE && stg != ST_TAKE && stg != ST_HUNGRY;
+        const unsigned mw = __ballot_sync(0xFFFFFFFFu, work);
+        const unsigned mo = __ballot_sync(0xFFFFFFFFu, stg == ST_TAKE || stg == ST_HUNGRY);
+        if (ln == 0) {
+          sh.mask[wid] = mw;
+          sh.mask2[wid] = mo;
+        }
+      }
+      __syncthreads();
+      const int pos = (tid & 31) * (BLOCK / 32) + (tid >> 5);
+      int item = -1, total = 0;
+#pragma unroll
+      for (int pass = 0; pass < 2; pass++)
+#pragma unroll
+        for (int w = 0; w < BLOCK / 32; w++) {
+          const unsigned mw = pass ? sh.mask2[w] : sh.mask[w];
+          const int c = __popc(mw);
+          if (item < 0 && pos < total + c) item = w * 32 + select_bit(mw, pos - total);
+          total += c;
+        }
+      if (item >= 0) {
+        Lane& L = sh.lane[item];
+        if (L.stage == ST_HUNGRY && sh.all_done) {
+          atomicAdd(&a.tasks->hungry, -1);
+          L.stage = ST_IDLE;
+        } else if (L.stage != ST_IDLE) {
+          DevEnv env = lane_env(sh, base + item, item);
+          if (env.tp && task_abandoned(L, env.tp)) abort_task(L, env);
+          const bool may_claim = L.stage == ST_HUNGRY && atomicSub(&sh.claim_slots, 1) > 0;
+          advance_free(L, env, a.free_steps, may_claim);
+        }
       }
       __syncthreads();
       if (tid == 0) {

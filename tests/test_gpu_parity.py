@@ -127,7 +127,9 @@ def test_ragged_batch_sizes(ddg, gpu_solver):
 
 @pytest.fixture(scope="module")
 def helper_solver(ddg):
-    s = ddg.Solver(tt_log2=10, jobs_per_deal=20, lanes=1024, block=256, min_blocks=2, help=1, time_limit_s=120)
+    # helpers in their own TTs (help_share_tt = -1); the shared-TT default is tested below
+    s = ddg.Solver(tt_log2=10, jobs_per_deal=20, lanes=1024, block=256, min_blocks=2, help=1, help_share_tt=-1,
+                   time_limit_s=120)
     yield s
     s.close()
 

@@ -1,0 +1,67 @@
+"""The serving load generator (dds_gpu_b200/serve.py): its seeded deal mix, and on the GPU a
+short run of Poisson arrivals through a stream whose every finished deal is checked
+against the reference's CPU solver (oracle/_ref, else the C restatement) here in the
+harness: continuous batching must not change a table."""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+P = ctypes.c_void_p
+
+
+def cpu_reference():
+    ref = os.path.join(ROOT, "oracle", "_ref", "libddref.so")
+    if os.path.exists(ref):
+        lib = ctypes.CDLL(ref)
+
+        def solve(h):
+            n = h.shape[0]
+            out = np.zeros(n * 20, np.int32)
+            assert lib.ref_solve_batch(h.ctypes.data_as(P), ctypes.c_long(n), 10, 8, out.ctypes.data_as(P), None) == 0
+            return out.reshape(n, 5, 4)
+        return solve
+    import subprocess
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
+    lib = ctypes.CDLL(os.path.join(ROOT, "oracle", "_build", "libddoracle.so"))
+    lib.ddo_solve_batch.restype = ctypes.c_longlong
+    lib.ddo_solve_batch.argtypes = [P, ctypes.c_long, ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P, P]
+
+    def solve(h):
+        n = h.shape[0]
+        out = np.zeros(n * 20, np.int32)
+        lib.ddo_solve_batch(h.ctypes.data, n, 10, 8, 5, None, out.ctypes.data, None)
+        return out.reshape(n, 5, 4)
+    return solve
+
+
+def test_mix_is_seeded_and_shaped(ddg):
+    from dds_gpu_b200 import serve
+    h, k = serve.mix_deals(7, 2000)
+    h2, k2 = serve.mix_deals(7, 2000)
+    assert (h == h2).all() and (k == k2).all()
+    assert 0.66 < (k == 13).mean() < 0.74
+    assert set(k[k < 13].tolist()) == {7, 8, 9, 10}
+    assert all(ddg.check_deal(x) for x in h[:200])
+    assert all(bin(int(x[0])).count("1") == kk for x, kk in zip(h, k))
+
+
+@pytest.mark.gpu
+def test_poisson_stream_matches_reference(ddg):
+    from dds_gpu_b200 import serve
+    s = ddg.Solver(tt_log2=10, jobs_per_deal=5, lanes=16384)
+    try:
+        r = serve.run_rate(s, rate=6.0, seconds=8.0, drain_s=20.0, sample_every=1, seed=11)
+    finally:
+        s.close()
+    assert r["arrived"] > 20 and r["admitted"] == r["arrived"]
+    hands, ks = serve.mix_deals(11, r["arrived"])
+    idx = sorted(r["sample"])
+    assert len(idx) >= r["arrived"] * 0.3  # the endings and the easier full deals finished
+    got = np.array([r["sample"][i] for i in idx], dtype=np.int32).reshape(-1, 5, 4)
+    want = cpu_reference()(np.ascontiguousarray(hands[idx]))
+    assert (got == want).all()
+    assert r["latency_ms"]["p50"] is not None
