@@ -19,6 +19,10 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "_lib", "libddg.so")
 # the same library built with bounds checks on every stack, TT and task index (tests)
 CHECK_LIB_PATH = os.path.join(_HERE, "_lib", "libddg_check.so")
+# the same library with 12-byte signature TT entries (the reference's DD_TT_SIG option): a
+# bucket of 256 bytes instead of 320, any number of relevant cards stored, not strictly
+# exact (a wrong hit needs two keys with the same tag and 64-bit hash)
+SIG_LIB_PATH = os.path.join(_HERE, "_lib", "libddg_sig.so")
 _lib = None
 _libs = {}
 
@@ -100,6 +104,7 @@ def load_library(path=None):
     lib.ddg_ns_tricks.argtypes = [P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                   ctypes.POINTER(ctypes.c_int)]
     lib.ddg_stream_open.argtypes = [P, ctypes.c_int, ctypes.c_double, ctypes.POINTER(P)]
+    lib.ddg_stream_open_guided.argtypes = [P, ctypes.c_int, ctypes.c_double, P, ctypes.POINTER(P)]
     lib.ddg_stream_submit.argtypes = [P, P, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]
     lib.ddg_stream_poll.argtypes = [P, P, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]
     lib.ddg_stream_in_flight.argtypes = [P]
@@ -280,10 +285,15 @@ class Stream:
     """Continuous batching on one solver (ddg_stream_*): submit deals while others are on
     the GPU, poll 28-byte records (index, 20 tricks) as deals finish, out of order."""
 
-    def __init__(self, solver, ring_slots=0, idle_timeout_s=0.0):
+    def __init__(self, solver, ring_slots=0, idle_timeout_s=0.0, guide=None):
+        """`guide`: a Guide on the solver's device whose seeds and root leads steer every
+        deal's search (the solver then needs at most (SMs - 2) * block lanes)."""
         self._lib = solver._lib
         self._h = P()
-        _check(self._lib.ddg_last_error, self._lib.ddg_stream_open(solver._h, ring_slots, idle_timeout_s, ctypes.byref(self._h)))
+        _check(self._lib.ddg_last_error,
+               self._lib.ddg_stream_open_guided(solver._h, ring_slots, idle_timeout_s,
+                                                guide._h if guide is not None else None, ctypes.byref(self._h)))
+        self._guide = guide  # kept alive while the stream uses it
         self.stats = None
 
     @property

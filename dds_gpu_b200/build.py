@@ -26,6 +26,8 @@ TARGETS = {
     "libddg.so": (["ddg_api.cu"], ["-shared"], "lib"),
     # the same library with every stack, TT and task index checked before use (tests)
     "libddg_check.so": (["ddg_api.cu"], ["-shared", "-DDDG_BOUNDS_CHECK"], "lib"),
+    # 12-byte signature TT entries (a speed option, not strictly exact)
+    "libddg_sig.so": (["ddg_api.cu"], ["-shared", "-DDDG_TT_SIG"], "lib"),
 }
 CLI = {
     "dd_gpu": "cli_dd_gpu.cpp",

@@ -78,8 +78,10 @@ struct ddg_solver {
 
 extern "C" {
 
-#ifdef DDG_BOUNDS_CHECK
+#if defined(DDG_BOUNDS_CHECK)
 const char* ddg_version(void) { return "ddg 0.2 (sm_100a, bounds-checked)"; }
+#elif defined(DDG_TT_SIG)
+const char* ddg_version(void) { return "ddg 0.2 (sm_100a, 12-byte signature TT entries, not strictly exact)"; }
 #else
 const char* ddg_version(void) { return "ddg 0.2 (sm_100a)"; }
 #endif
@@ -571,6 +573,10 @@ int ddg_solve_continue(ddg_solver* s, double seconds, const uint64_t* hands_host
 
 // ---- streams: a device ring of deals fed while the persistent kernel runs ---------------
 
+// The guide's inference on `stream` (ddg_guide_api.cuh): seeds and root leads of n deals.
+static int guide_predict_on(ddg_guide* g, const uint64_t* d_hands, int64_t n, int8_t* d_seed20, int8_t* d_hint20,
+                            cudaStream_t stream);
+
 struct ddg_stream {
   ddg_solver* s = nullptr;
   int slots = 0;
@@ -587,6 +593,9 @@ struct ddg_stream {
   unsigned long long published = 0, consumed = 0;
   cudaStream_t kstream = nullptr, cstream = nullptr;
   cudaEvent_t kdone = nullptr;
+  ddg_guide* guide = nullptr;             // guided stream: seeds and root leads per ring slot
+  int8_t* d_seed = nullptr;
+  int8_t* d_hint = nullptr;
   bool launched = false;
   double idle_timeout_s = 30;
   int launches = 0;
@@ -598,6 +607,8 @@ static void stream_free(ddg_stream* st) {
   cudaFree(st->d_ring);
   cudaFree(st->d_out);
   cudaFree(st->d_done);
+  cudaFree(st->d_seed);
+  cudaFree(st->d_hint);
   cudaFree(st->d_words);
   if (st->h_comp) cudaFreeHost(st->h_comp);
   if (st->h_stage) cudaFreeHost(st->h_stage);
@@ -636,6 +647,11 @@ static int stream_kernel(ddg_stream* st) {
   a.ring_mask = st->slots - 1;
   a.idle_ns = (u64)(st->idle_timeout_s * 1e9);
   a.n_jobs = 0;
+  if (st->guide) {  // each slot's NS seeds (stepping search) and root leads, written at submit
+    a.mode = MODE_STEP;
+    a.seeds = st->d_seed;
+    a.hint20 = st->d_hint;
+  }
   *(volatile int*)s->h_stop = 0;
   int grid = 0;
   int rc = launch_batch(s, a, (long long)s->lanes, st->kstream, &grid);
@@ -647,9 +663,19 @@ static int stream_kernel(ddg_stream* st) {
 }
 
 int ddg_stream_open(ddg_solver* s, int ring_slots, double idle_timeout_s, ddg_stream** out) {
+  return ddg_stream_open_guided(s, ring_slots, idle_timeout_s, nullptr, out);
+}
+
+int ddg_stream_open_guided(ddg_solver* s, int ring_slots, double idle_timeout_s, ddg_guide* guide,
+                           ddg_stream** out) {
   if (!out) return fail(DDG_E_ARG, "null output");
   *out = nullptr;
   if (!s) return fail(DDG_E_ARG, "null solver");
+  if (guide && (s->lanes + s->block - 1) / s->block > s->sms - 2)
+    return fail(DDG_E_STATE,
+                "a guided stream needs SMs the solver leaves free for the guide's kernels: create the solver "
+                "with lanes <= (SMs - 2) * block = %d",
+                (s->sms - 2) * s->block);
   if (s->streaming) return fail(DDG_E_STATE, "a stream is already open on this solver");
   if (s->cfg.schedule == 1) return fail(DDG_E_ARG, "streams run on the block-phase kernel (schedule 0 or 2)");
   if (ring_slots <= 0) ring_slots = 65536;
@@ -678,6 +704,11 @@ int ddg_stream_open(ddg_solver* s, int ring_slots, double idle_timeout_s, ddg_st
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&st->kstream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&st->cstream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&st->kdone, cudaEventDisableTiming);
+  if (e == cudaSuccess && guide) {
+    st->guide = guide;
+    e = cudaMalloc(&st->d_seed, (size_t)ring_slots * 20);
+    if (e == cudaSuccess) e = cudaMalloc(&st->d_hint, (size_t)ring_slots * 20);
+  }
   if (e == cudaSuccess) e = cudaMemset(st->d_done, 0, (size_t)ring_slots * 4);
   if (e == cudaSuccess) e = cudaMemset(st->d_words, 0, 4 * 8);
   if (e == cudaSuccess) e = cudaMemset(s->counters, 0, CNT_WORDS * 8);
@@ -727,6 +758,16 @@ int ddg_stream_submit(ddg_stream* st, const uint64_t* hands, int64_t n, int64_t*
                              st->cstream));
     if ((unsigned long long)k > run1)
       CUDA_TRY(cudaMemcpyAsync(st->d_ring, st->h_stage, (k - run1) * 32, cudaMemcpyHostToDevice, st->cstream));
+    if (st->guide) {  // the guide's seeds and leads for the new slots, before they are published
+      int rc = guide_predict_on(st->guide, st->d_ring + first * 4, (int64_t)run1, st->d_seed + first * 20,
+                                st->d_hint + first * 20, st->cstream);
+      if (rc == DDG_OK && (unsigned long long)k > run1)
+        rc = guide_predict_on(st->guide, st->d_ring, (int64_t)(k - run1), st->d_seed, st->d_hint, st->cstream);
+      if (rc) {
+        for (int64_t i = 0; i < k; i++) st->slot_busy[(st->published + i) & mask] = 0;
+        return rc;
+      }
+    }
     st->h_words[0] = st->published + k;  // published after the deals (same copy stream)
     CUDA_TRY(cudaMemcpyAsync(st->d_words + 0, st->h_words + 0, 8, cudaMemcpyHostToDevice, st->cstream));
     CUDA_TRY(cudaStreamSynchronize(st->cstream));

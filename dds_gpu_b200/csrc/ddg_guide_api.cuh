@@ -277,22 +277,41 @@ int ddg_guide_predict(ddg_guide* g, const uint64_t* d_hands, int64_t n, int8_t* 
   if (!g || (n > 0 && !d_hands)) return fail(DDG_E_ARG, "null argument");
   if (n < 0) return fail(DDG_E_ARG, "n < 0");
   CUDA_TRY(cudaSetDevice(g->device));
-  CUDA_TRY(cudaMemset(g->err, 0, 4));
+  int rc = guide_predict_on(g, d_hands, n, d_seed20, d_hint20, nullptr);
+  if (rc) return rc;
+  CUDA_TRY(cudaDeviceSynchronize());
+  return check_err(g);
+}
+
+}  // extern "C"
+
+// The inference of ddg_guide_predict on `stream`, waiting for that stream only: a guided
+// stream calls it while its persistent solve kernel runs on another stream.
+static int guide_predict_on(ddg_guide* g, const uint64_t* d_hands, int64_t n, int8_t* d_seed20, int8_t* d_hint20,
+                            cudaStream_t stream) {
+  using namespace guide_nn;
+  CUDA_TRY(cudaMemsetAsync(g->err, 0, 4, stream));
   const int64_t total = n * 20;
   for (int64_t first = 0; first < total; first += g->max_rows) {
     const int rows = (int)std::min<int64_t>(g->max_rows, total - first);
     const int R = (rows + TILE_M - 1) / TILE_M * TILE_M;
     std::vector<int64_t> idx(R, -1);
     for (int i = 0; i < rows; i++) idx[i] = first + i;
-    CUDA_TRY(cudaMemcpy(g->rows_buf, idx.data(), (size_t)R * 8, cudaMemcpyHostToDevice));
-    features<<<R, 64>>>(d_hands, g->rows_buf, R, g->X);
-    int rc = forward(g, R, nullptr);
+    // from pageable memory: the call returns once the rows are staged, so idx may go
+    CUDA_TRY(cudaMemcpyAsync(g->rows_buf, idx.data(), (size_t)R * 8, cudaMemcpyHostToDevice, stream));
+    features<<<R, 64, 0, stream>>>(d_hands, g->rows_buf, R, g->X);
+    int rc = forward(g, R, stream);
     if (rc) return rc;
-    predict_out<<<(rows + 127) / 128, 128>>>(g->L, d_hands, first, rows, d_seed20, d_hint20);
+    predict_out<<<(rows + 127) / 128, 128, 0, stream>>>(g->L, d_hands, first, rows, d_seed20, d_hint20);
     CUDA_TRY(cudaGetLastError());
   }
-  CUDA_TRY(cudaDeviceSynchronize());
-  return check_err(g);
+  if (stream) {
+    CUDA_TRY(cudaStreamSynchronize(stream));
+    return check_err(g);
+  }
+  return DDG_OK;
 }
+
+extern "C" {
 
 }  // extern "C"

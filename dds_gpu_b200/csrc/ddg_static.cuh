@@ -31,7 +31,9 @@ constexpr size_t OFF_STACKS = round256(TT_BYTES);
 constexpr size_t OFF_GEN = OFF_STACKS + round256(STACK_BYTES);
 constexpr size_t OFF_CNT = OFF_GEN + round256(GEN_BYTES);
 constexpr size_t SCRATCH_BYTES = OFF_CNT + round256(CNT_BYTES);
+#ifndef DDG_TT_SIG
 static_assert(SCRATCH_BYTES / 100000 == 426, "the scratch size stated in ddg.h is 42.6 MB");
+#endif
 
 static __device__ __align__(256) unsigned char g_scratch[SCRATCH_BYTES];
 

@@ -1,7 +1,7 @@
 """Serving load generator for the streaming solver (continuous batching, ddg_stream_*).
 
-    python -m dds_gpu_b200.serve [--seconds 120] [--fractions 0.25,0.5,0.75,1.0] [--guide]
-                                 [--out FILE] [--sample-every 50]
+    python -m dds_gpu_b200.serve [--seconds 120] [--fractions 0.25,0.5,0.75,1.0]
+                                 [--modes plain,guided] [--out FILE] [--sample-every 50]
 
 Workload: a seeded mix of 70 % random 13-card deals and 30 % K-card endings, K uniform in
 7..10, arriving as a Poisson process at fractions of the measured capacity. Capacity is
@@ -16,7 +16,9 @@ For each rate: deals arrive for --seconds; solved rate, in-flight deals (sampled
 second) and the latency of every deal from its arrival to its result on the host, with
 p50 / p99 / p99.9 over the deals that arrived in the second half of the window (after the
 start-up) and finished before the drain limit; deals still running then are counted, not
-guessed. Every --sample-every-th deal's table is kept (deal, table) for checking.
+guessed. Every --sample-every-th deal's table is kept (deal, table) for checking. Each
+rate runs plain (DDS order, binary search) and guided (the learned guide's seeds and root
+leads, computed on the GPU as deals are submitted), on the same lanes.
 """
 import argparse
 import json
@@ -55,7 +57,7 @@ def capacity(solver, seconds, torch):
     return st["nodes"] / (st["kernel_ms"] * 1e-3)
 
 
-def run_rate(solver, rate, seconds, drain_s, sample_every, seed):
+def run_rate(solver, rate, seconds, drain_s, sample_every, seed, guide=None):
     rng = np.random.default_rng(seed)
     gaps = rng.exponential(1.0 / rate, int(rate * seconds * 1.5) + 100)
     arrivals = np.cumsum(gaps)
@@ -64,7 +66,7 @@ def run_rate(solver, rate, seconds, drain_s, sample_every, seed):
     hands, ks = mix_deals(seed, n)
     done_at = np.full(n, np.nan)
     sample = {}
-    st = Stream(solver, ring_slots=65536, idle_timeout_s=5)
+    st = Stream(solver, ring_slots=65536, idle_timeout_s=5, guide=guide)
     in_flight = []
     submitted = 0
     t0 = time.perf_counter()
@@ -123,9 +125,15 @@ def main(argv=None):
     p.add_argument("--nodes-per-deal", type=float, default=NODES_PER_DEAL)
     p.add_argument("--capacity", type=float, default=0.0, help="deals/s at full load (0 = measure it)")
     p.add_argument("--sample-every", type=int, default=50)
+    p.add_argument("--modes", default="plain,guided", help="plain and/or guided (the learned guide in the stream)")
     p.add_argument("--out", default="")
     a = p.parse_args(argv)
-    solver = Solver(tt_log2=10, jobs_per_deal=5)
+    from . import Guide
+    from .guide import load_weights
+    # Both modes run on the same lanes: a guided stream leaves two SMs to the guide's kernels.
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    solver = Solver(tt_log2=10, jobs_per_deal=5, lanes=(sms - 2) * 512)
+    guide = None
     try:
         cap = a.capacity
         rep = {"workload": "70% random 13-card deals + 30% K=7..10 endings, seeded, Poisson arrivals",
@@ -136,12 +144,23 @@ def main(argv=None):
             rep["capacity_nodes_per_s"] = nps
         rep["capacity_deals_per_s"] = cap
         rep["rates"] = []
+        modes = a.modes.split(",")
+        params = load_weights() if "guided" in modes else None
+        if params is not None:
+            guide = Guide(device=0, max_rows=4096, params=params)
         for i, f in enumerate(float(x) for x in a.fractions.split(",")):
-            r = run_rate(solver, f * cap, a.seconds, a.drain, a.sample_every, MIX_SEED + 100 + i)
-            r["fraction"] = f
-            rep["rates"].append(r)
-            print(json.dumps({k: v for k, v in r.items() if k != "sample"}), flush=True)
+            for mode in modes:
+                if mode == "guided" and guide is None:
+                    continue
+                r = run_rate(solver, f * cap, a.seconds, a.drain, a.sample_every, MIX_SEED + 100 + i,
+                             guide if mode == "guided" else None)
+                r["fraction"] = f
+                r["mode"] = mode
+                rep["rates"].append(r)
+                print(json.dumps({k: v for k, v in r.items() if k != "sample"}), flush=True)
     finally:
+        if guide is not None:
+            guide.close()
         solver.close()
     if a.out:
         with open(a.out, "w") as f:

@@ -32,6 +32,7 @@ extern "C" {
 #define DDG_E_TIMEOUT -5 /* a bounded device wait gave up */
 
 typedef struct ddg_solver ddg_solver;
+typedef struct ddg_guide ddg_guide; /* the learned guide (below) */
 
 /* Solver configuration. Zero fields take the defaults. Mirrors the reference's knobs:
  * TT_LOG2 (gpu/gpu_main.cu:192), THREADS (:202), PER_LEAD (gpu/stream_main.cu:167),
@@ -188,6 +189,13 @@ int ddg_solve_begin_ex(ddg_solver* s, const uint64_t* d_hands, int64_t n, const 
  * calls return DDG_E_STATE. Runs on the block-phase kernel (schedule 0 or 2), helping off. */
 typedef struct ddg_stream ddg_stream;
 int ddg_stream_open(ddg_solver* s, int ring_slots, double idle_timeout_s, ddg_stream** out);
+/* A stream whose deals are searched with the learned guide (`guide`, on the solver's
+ * device): every submit runs the guide on the new deals before they are published, and
+ * each job steps from the guide's NS seed with its lead tried first at the root, as
+ * ddg_solve_device_ex. The guide's kernels need SMs the persistent solve kernel leaves
+ * free: the solver must have at most (SMs - 2) * block lanes (else DDG_E_STATE). */
+int ddg_stream_open_guided(ddg_solver* s, int ring_slots, double idle_timeout_s, ddg_guide* guide,
+                           ddg_stream** out);
 int ddg_stream_submit(ddg_stream* st, const uint64_t* hands, int64_t n, int64_t* accepted);
 /* Copies up to `max` finished deals' 28-byte records into rec28; *got = how many. */
 int ddg_stream_poll(ddg_stream* st, uint8_t* rec28, int64_t max, int64_t* got);
@@ -223,7 +231,6 @@ int ddg_ns_tricks(ddg_solver* s, const uint64_t* hands4, int strain, int leader,
  * fp32 array of ddg_guide_param_count() values: W1[256][256] (inputs padded to 256),
  * b1[256], W2[256][256], b2[256], W3[80][256] (outputs padded to 80), b3[80]. An example
  * is (deal, strain, declarer) = index deal*20 + strain*4 + declarer, leader = declarer+1. */
-typedef struct ddg_guide ddg_guide;
 int64_t ddg_guide_param_count(void);
 /* max_rows: examples per training step / inference pass, a multiple of 128. params: the
  * initial parameters (NULL = zeros). */

@@ -20,6 +20,11 @@ g++ -O3 -std=c++17 -march=x86-64-v3 -pthread -fPIC -shared -I"$REF_DIR/src" \
   -o "$OUT/libddref.so.tmp" "$HERE/ref_shim.cpp"
 mv "$OUT/libddref.so.tmp" "$OUT/libddref.so"
 echo "built $OUT/libddref.so"
+# The same with the reference's 12-byte signature entries (-DDD_TT_SIG, src/dd.h:74-85).
+g++ -O3 -std=c++17 -march=x86-64-v3 -pthread -fPIC -shared -DDD_TT_SIG -I"$REF_DIR/src" \
+  -o "$OUT/libddref_sig.so.tmp" "$HERE/ref_shim.cpp"
+mv "$OUT/libddref_sig.so.tmp" "$OUT/libddref_sig.so"
+echo "built $OUT/libddref_sig.so"
 g++ -O3 -std=c++17 -march=x86-64-v3 -pthread -DWITH_REF -I"$REF_DIR/src" \
   -o "$OUT/cpu_window.tmp" "$HERE/cpu_window.cpp"
 mv "$OUT/cpu_window.tmp" "$OUT/cpu_window"

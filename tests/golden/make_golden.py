@@ -3,6 +3,7 @@
 
     python tests/golden/make_golden.py          # all fixtures
     python tests/golden/make_golden.py mixed    # only the uneven-hardness one
+    python tests/golden/make_golden.py sig      # only the signature-entry ones
 
 Each fixture holds seeded deals (tests/golden/deals_np.py), the reference's trick tables
 (dd_solve_strain, src/dd.h:926) and its search-node count per job, with one job per
@@ -78,11 +79,32 @@ def mixed_fixture(name, seed, n, k_min=5, k_max=13, skew=0.3, tt_log2=10):
     print(name, n, "deals", int(n5.sum()), "nodes")
 
 
+def sig_fixtures():
+    """The reference built with its 12-byte signature entries (-DDD_TT_SIG,
+    oracle/_ref/libddref_sig.so): tricks and per-job nodes of endings and light full deals."""
+    sig = ctypes.CDLL(os.path.join(ROOT, "oracle", "_ref", "libddref_sig.so"))
+    for name, h in (("sig_k6_120.npz", make_deals(106, 0, 120, 6)), ("sig_k9_120.npz", make_deals(109, 0, 120, 9)),
+                    ("sig_k13_5.npz", make_deals(2, 0, 24, 13)[[1, 3, 15, 17, 22]])):
+        h = np.ascontiguousarray(h)
+        n = h.shape[0]
+        out = np.zeros(n * 20, np.int32)
+        nodes = np.zeros(n * 5, np.uint64)
+        assert sig.ref_solve_batch(h.ctypes.data_as(P), ctypes.c_long(n), 10, 8, out.ctypes.data_as(P),
+                                   nodes.ctypes.data_as(P)) == 0
+        t = out.reshape(n, 5, 4).astype(np.uint8)
+        exact, _ = ref_solve(h)
+        assert (t == exact).all()  # no signature collision on these deals
+        np.savez_compressed(os.path.join(HERE, name), tt_log2=10, hands=h, tricks=t, nodes_jpd5=nodes.astype(np.uint32))
+        print(name, n, "deals", int(nodes.sum()), "nodes (signature entries)")
+
+
 def main():
     only = sys.argv[1:]
     if only:  # regenerate the named fixtures only
         if "mixed" in only:
             mixed_fixture("mixed_300.npz", seed=3000, n=300)
+        if "sig" in only:
+            sig_fixtures()
         return
     # Config 1: K=6 endings, 4096 deals, TT_LOG2=10.
     fixture("k6_4096.npz", seed=1, n=4096, k=6)
@@ -108,6 +130,8 @@ def main():
     print("k8_200_seeded.npz", int(ng.sum()), "nodes")
     # Uneven-hardness deals, K = 5..13, 30 % skewed.
     mixed_fixture("mixed_300.npz", seed=3000, n=300)
+    # The signature-entry build of the reference.
+    sig_fixtures()
 
 
 if __name__ == "__main__":

@@ -65,3 +65,35 @@ def test_poisson_stream_matches_reference(ddg):
     want = cpu_reference()(np.ascontiguousarray(hands[idx]))
     assert (got == want).all()
     assert r["latency_ms"]["p50"] is not None
+
+
+@pytest.mark.gpu
+def test_guided_stream_matches_reference(ddg):
+    """The learned guide inside a stream (seeds and root leads computed as deals are
+    submitted, while the persistent solve kernel runs): same tables as the reference."""
+    import torch
+    from dds_gpu_b200 import guide as ddg_guide
+    from dds_gpu_b200 import serve
+    params = ddg_guide.load_weights()
+    if params is None:
+        pytest.skip("no guide weights file")
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    full = ddg.Solver(tt_log2=10, jobs_per_deal=5)
+    g = ddg.Guide(device=0, max_rows=4096, params=params)
+    try:
+        with pytest.raises(ddg.DDGError):  # no SM left for the guide's kernels
+            ddg.Stream(full, ring_slots=64, guide=g)
+        full.close()
+        s = ddg.Solver(tt_log2=10, jobs_per_deal=5, lanes=(sms - 2) * 512)
+        try:
+            r = serve.run_rate(s, rate=6.0, seconds=8.0, drain_s=20.0, sample_every=1, seed=12, guide=g)
+        finally:
+            s.close()
+    finally:
+        g.close()
+        full.close()
+    hands, _ = serve.mix_deals(12, r["arrived"])
+    idx = sorted(r["sample"])
+    assert len(idx) >= r["arrived"] * 0.3
+    got = np.array([r["sample"][i] for i in idx], dtype=np.int32).reshape(-1, 5, 4)
+    assert (got == cpu_reference()(np.ascontiguousarray(hands[idx]))).all()
