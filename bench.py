@@ -327,7 +327,8 @@ def our_arm(a, rank, world, local_rank):
         if rank == 0:
             print(json.dumps({"profile_case": True, "launches": a.warmup + 1, "last_launch": {
                 k: st[k] for k in ("nodes", "tt_probes", "tt_entry_reads", "tt_stores", "tt_bytes", "kernel_ms",
-                                   "lanes", "grid", "block", "jobs_done")}}), flush=True)
+                                   "lanes", "grid", "block", "jobs_done", "enter_exit", "phase_warps", "phase_items",
+                                   "phase_cycles", "free_rounds", "free_cycles", "iterations")}}), flush=True)
         solver.close()
         return
 

@@ -5,13 +5,14 @@
 Workload: (deal, strain) jobs over deals from ddg_make_deals_mixed (K uniform in 5..13
 cards per seat, 30 % skewed with a 7-10 card suit facing a void), seed 7.
 
-The tuner sweeps the launch shape (512 threads x 1 block or 256 x 2 per SM), solver lanes,
-TT size (2^9..2^12 buckets per lane) and the kernel's stage schedule (block phases or
-per-warp queues); each candidate runs a short resumable slice
-of the same set and is scored by the search nodes it covers per second. The chosen
-setting then solves the whole set as one CUDA-graph launch of the persistent kernel
-(helping on with the block-phase kernel, so idle lanes split the last hard jobs), with
-per-job completion times for the tail.
+The tuner sweeps the launch shape (512 threads x 1 block or 256 x 2 per SM), solver lanes
+and the kernel's stage schedule (block phases or per-warp queues) at one TT size; each
+candidate runs a short resumable slice of the same set and is scored by the search nodes
+it covers per second. The TT size (2^9..2^12 buckets per lane) is then the largest that
+fits beside the chosen lanes (tune() says why node rates do not rank TT sizes). The
+chosen setting then solves the whole set as one CUDA-graph launch of the persistent kernel
+(optionally with helping: idle lanes split the last hard jobs in shared TTs; --help-lanes),
+with per-job completion times for the tail.
 """
 import argparse
 import itertools
@@ -50,9 +51,16 @@ def measure(cfg, d_hands, n, window_s, torch):
 
 
 def tune(d_hands, n, window_s, torch, log=print):
+    """Launch shape, lanes and stage schedule by node rate at one TT size (a job then costs
+    the same nodes in every candidate, so nodes per second compares them fairly); then the
+    TT size: the largest of TT_LOG2 that fits beside the chosen lanes. Node rates of other
+    TT sizes are not comparable (a larger table answers more positions, so the same job
+    takes fewer nodes: 1.5-2.5x fewer for hard 13-card jobs at 2^12 than at 2^10, at about
+    the same node rate), so they are measured and reported, not used to rank."""
     results = []
-    for (block, minb), lanes, tt, sch in itertools.product(SHAPES, LANES, TT_LOG2, SCHEDULES):
-        cfg = {"block": block, "min_blocks": minb, "lanes": lanes, "tt_log2": tt, "schedule": sch}
+    base_tt = 10 if 10 in TT_LOG2 else TT_LOG2[0]
+    for (block, minb), lanes, sch in itertools.product(SHAPES, LANES, SCHEDULES):
+        cfg = {"block": block, "min_blocks": minb, "lanes": lanes, "tt_log2": base_tt, "schedule": sch}
         try:
             rate, jobs_rate, used = measure(cfg, d_hands, n, window_s, torch)
         except DDGError as e:  # e.g. the TTs do not fit
@@ -61,17 +69,33 @@ def tune(d_hands, n, window_s, torch, log=print):
         cfg["lanes"] = used
         cfg["jobs_per_s"] = jobs_rate
         results.append((rate, cfg))
-        log(f"  block {block}x{minb} lanes {used:6d} TT 2^{tt} schedule {sch}: {rate / 1e6:7.1f} M nodes/s, "
+        log(f"  block {block}x{minb} lanes {used:6d} TT 2^{base_tt} schedule {sch}: {rate / 1e6:7.1f} M nodes/s, "
             f"{jobs_rate:9.1f} jobs/s")
     results.sort(key=lambda r: -r[0])
-    return results[0][1], results
+    best = dict(results[0][1])
+    for tt in sorted(TT_LOG2, reverse=True):
+        cfg = dict(best, tt_log2=tt)
+        try:
+            rate, jobs_rate, used = measure(cfg, d_hands, n, window_s, torch)
+        except DDGError as e:
+            log(f"  TT 2^{tt}: {e}")
+            continue
+        if used < best["lanes"]:  # the larger tables do not fit beside the chosen lanes
+            log(f"  TT 2^{tt}: only {used} lanes fit")
+            continue
+        cfg["jobs_per_s"] = jobs_rate
+        results.append((rate, cfg))
+        log(f"  TT 2^{tt} at the chosen shape: {rate / 1e6:7.1f} M nodes/s")
+        best = cfg
+        break
+    return best, results
 
 
-def run_batch(cfg, d_hands, n, limit_s, torch, tables=False):
+def run_batch(cfg, d_hands, n, limit_s, torch, tables=False, help=False):
     """The whole set as one graph-launched persistent solve; completion-time tail (and the
     tables, (n, 5, 4) uint8 with 255 = unsolved, under "tables" when asked)."""
     s = Solver(tt_log2=cfg["tt_log2"], lanes=cfg["lanes"], block=cfg["block"], min_blocks=cfg["min_blocks"],
-               jobs_per_deal=5, schedule=cfg["schedule"], help=1 if cfg["schedule"] != 1 else 0,
+               jobs_per_deal=5, schedule=cfg["schedule"], help=1 if help and cfg["schedule"] != 1 else 0,
                time_limit_s=limit_s)
     try:
         d_out = torch.empty(n * 20, dtype=torch.uint8, device=d_hands.device)
@@ -105,6 +129,7 @@ def main():
     p.add_argument("--jobs", type=int, default=200000, help="(deal, strain) jobs: deals = jobs / 5")
     p.add_argument("--window", type=float, default=3.0, help="tuning slice per candidate, seconds")
     p.add_argument("--limit", type=float, default=300.0, help="time limit of the full batch, seconds")
+    p.add_argument("--help-lanes", action="store_true", help="idle lanes help with the last hard jobs")
     p.add_argument("--out", default="")
     a = p.parse_args()
     n = a.jobs // 5
@@ -114,9 +139,10 @@ def main():
     best, results = tune(d_hands, n, a.window, torch)
     print(f"autotuner ({time.time() - t0:.0f} s): block {best['block']}x{best['min_blocks']}, lanes {best['lanes']}, "
           f"TT 2^{best['tt_log2']}, schedule {best['schedule']}", flush=True)
-    rep = run_batch(best, d_hands, n, a.limit, torch)
+    rep = run_batch(best, d_hands, n, a.limit, torch, help=a.help_lanes)
     rep.update({"workload": f"{n} deals from ddg_make_deals_mixed(seed {SEED}, K 5..13, 30% skewed), "
-                            f"{a.jobs} (deal, strain) jobs, one CUDA-graph launch, helping on",
+                            f"{a.jobs} (deal, strain) jobs, one CUDA-graph launch, "
+                            f"helping {'on' if a.help_lanes else 'off'}",
                 "autotuner_choice": best,
                 "autotuner_table": [{"nodes_per_s": r, **c} for r, c in results]})
     print(json.dumps(rep), flush=True)

@@ -366,10 +366,26 @@ __device__ __forceinline__ void run_phase(BlockShared<BLOCK>& sh, long long base
   const int wid = tid >> 5, ln = tid & 31;
   const Lane& me = sh.lane[tid];
   bool want;
-  if (PH == PH_CHEAP)  // hungry lanes only when a task may be waiting (or to stop them)
+  if (PH == PH_CHEAP) {  // hungry lanes only when a task may be waiting (or to stop them)
     want = (cheap_stage(me.stage) && (me.stage != ST_HUNGRY || sh.claim_slots > 0 || sh.all_done)) ||
            (sh.args.tasks && task_abandoned(me, sh.args.tasks));
-  else if (PH == PH_LEAD) want = me.stage == ST_ENTER && me.p.nplayed == 0;
+    if (sh.args.ring) {
+      // Stream: of the lanes waiting for a job, only as many as the block may take this
+      // iteration poll the ring; the others stay out of the pass instead of each reading
+      // the published and taken counts in global memory.
+      const bool waiting = me.stage == ST_TAKE;
+      const unsigned mt = __ballot_sync(0xFFFFFFFFu, waiting);
+      if (ln == 0) sh.mask2[wid] = mt;
+      __syncthreads();
+      if (waiting) {
+        int rank = __popc(mt & ((1u << ln) - 1));
+        for (int w = 0; w < wid; w++) rank += __popc(sh.mask2[w]);
+        want = rank < sh.take_budget;
+      }
+    }
+  } else if (PH == PH_LEAD) {
+    want = me.stage == ST_ENTER && me.p.nplayed == 0;
+  }
   else if (PH == PH_FOLLOW) want = me.stage == ST_ENTER && me.p.nplayed != 0;
   else if (PH == PH_MOVES_LEAD) want = me.stage == ST_MOVES_LEAD;
   else want = me.stage == ST_MOVES_FOLLOW;
