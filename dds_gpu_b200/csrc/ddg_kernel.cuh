@@ -84,6 +84,7 @@ struct BatchArgs {
   // `one_strain` of deal 0, for declarer `one_decl` alone (-1 = all four). A zeroed
   // BatchArgs has it off. `first_target` is the binary search's first target (0 = 7).
   int one_job, one_strain, one_decl, first_target;
+  int flat_moves;        // the lead-move phase spreads (lane, candidate) pairs over the block
 };
 
 // One finished deal of a stream: its sequence number and table; `flag` = record index + 1,
@@ -312,6 +313,12 @@ struct BlockShared {
   BatchArgs args;
   unsigned mask[BLOCK / 32];
   unsigned mask2[BLOCK / 32];  // free-running rounds: lanes waiting for a job or a task
+  // flattened lead-move phase (run_moves_lead_flat), per position of the phase's list
+  u64 fl_cand[BLOCK], fl_all[BLOCK];
+  uint16_t fl_item[BLOCK], fl_off[BLOCK];
+  int8_t fl_hint[BLOCK];
+  int fl_wsum[BLOCK / 32];
+  int16_t fl_score[BLOCK * 13];
   unsigned long long ph_warps[PH_COUNT], ph_items[PH_COUNT], iters;
   int stop;
   int help_hint;    // hungry lanes outnumber queued tasks (read once per iteration)
@@ -431,6 +438,104 @@ __device__ __forceinline__ void run_phase(BlockShared<BLOCK>& sh, long long base
       step_moves(L, env);
       step_next(L, env);  // a fresh node plays its first candidate (never a skipped one)
     }
+  }
+  __syncthreads();
+}
+
+// The lead-move phase with its work flattened: every (lane, candidate) pair of the phase
+// is one item, and the items are spread over all threads of the block, so the DDS lead
+// weights of one lane's candidates are computed side by side instead of in a loop whose
+// length differs from lane to lane of a warp. Each lane's thread then orders its
+// candidates exactly as gen_moves_lead does (arrival order highest card first, stable by
+// weight), so the search and its node counts are unchanged.
+template <int BLOCK>
+__device__ __forceinline__ void run_moves_lead_flat(BlockShared<BLOCK>& sh, long long base, int tid) {
+  const int wid = tid >> 5, ln = tid & 31;
+  const bool want = sh.lane[tid].stage == ST_MOVES_LEAD;
+  const unsigned m = __ballot_sync(0xFFFFFFFFu, want);
+  if (ln == 0) sh.mask[wid] = m;
+  __syncthreads();
+  int total = 0, item = -1;
+#pragma unroll
+  for (int w = 0; w < BLOCK / 32; w++) {
+    const unsigned mw = sh.mask[w];
+    const int c = __popc(mw);
+    if (item < 0 && tid < total + c) item = w * 32 + select_bit(mw, tid - total);
+    total += c;
+  }
+  // 1. each item's candidates (and the root hint, as step_moves takes it)
+  int cnt = 0;
+  u64 cand = 0;
+  DevEnv env;
+  if (item >= 0) {
+    env = lane_env(sh, base + item, item);
+    const Lane& L = sh.lane[item];
+    int hint = frame_hint(L.f);
+    if (hint < 0 && L.sp == 0 && L.task < 0) {
+      const int h = env.root_hint(L);
+      if (h >= 0 && h < 64 && (hand_at(L.p.h, L.p.leader) >> h & 1)) hint = h;
+    }
+    u64 all;
+    cand = candidates(L.p, L.p.leader, all);
+    cnt = popc(cand);
+    sh.fl_cand[tid] = cand;
+    sh.fl_all[tid] = all;
+    sh.fl_item[tid] = (uint16_t)item;
+    sh.fl_hint[tid] = (int8_t)hint;
+  }
+  // 2. where each item's candidates start in the flat list (exclusive prefix sum)
+  int incl = cnt;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const int v = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+    if (ln >= d) incl += v;
+  }
+  if (ln == 31) sh.fl_wsum[wid] = incl;
+  __syncthreads();
+  int off = incl - cnt, work = 0;
+#pragma unroll
+  for (int w = 0; w < BLOCK / 32; w++) {
+    if (w < wid) off += sh.fl_wsum[w];
+    work += sh.fl_wsum[w];
+  }
+  if (item >= 0) sh.fl_off[tid] = (uint16_t)off;
+  __syncthreads();
+  // 3. the weights, one (lane, candidate) pair per thread at a time
+  for (int w = tid; w < work; w += BLOCK) {
+    int lo = 0, hi = total - 1;  // the last item whose candidates start at or before w
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (sh.fl_off[mid] <= w) lo = mid;
+      else hi = mid - 1;
+    }
+    u64 rest = sh.fl_cand[lo];
+    for (int k = w - sh.fl_off[lo]; k > 0; k--) rest ^= card_bit(top_bit(rest));
+    const int card = top_bit(rest);
+    const Lane& L = sh.lane[sh.fl_item[lo]];
+    Hands hs;
+    for (int i = 0; i < 4; i++) hs.h[i] = L.p.h[i];
+    const int hint = sh.fl_hint[lo];
+    const bool hinted = hint >= 0 && alike(hand_at(L.p.h, L.p.leader), sh.fl_all[lo], hint, card);
+    sh.fl_score[w] = (int16_t)lead_weight(hs, L.top, L.p.trump, L.p.left, L.p.leader, card, hinted);
+  }
+  __syncthreads();
+  // 4. each lane's candidates ordered as gen_moves_lead orders them, then its first move
+  if (item >= 0) {
+    Lane& L = sh.lane[item];
+    int n = 0, score[13], card_of[13];
+    u64 rest = cand;
+    for (int k = 0; k < cnt; k++) {
+      const int card = top_bit(rest);
+      rest ^= card_bit(card);
+      insert_move(score, card_of, n, card, sh.fl_score[off + k]);
+    }
+    pack_moves(L.f, card_of, n);
+    L.stage = ST_NEXT;
+    step_next(L, env);
+  }
+  if (tid == 0 && total) {
+    sh.ph_items[PH_MOVES_LEAD] += total;
+    sh.ph_warps[PH_MOVES_LEAD] += (total + 31) >> 5;
   }
   __syncthreads();
 }
@@ -565,7 +670,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(BatchArgs a) {
     long long t2 = clock64();
     run_phase<BLOCK, PH_FOLLOW>(sh, base, tid);
     long long t3 = clock64();
-    run_phase<BLOCK, PH_MOVES_LEAD>(sh, base, tid);
+    if (sh.args.flat_moves) run_moves_lead_flat<BLOCK>(sh, base, tid);
+    else run_phase<BLOCK, PH_MOVES_LEAD>(sh, base, tid);
     long long t4 = clock64();
     run_phase<BLOCK, PH_MOVES_FOLLOW>(sh, base, tid);
     if (tid == 0) {

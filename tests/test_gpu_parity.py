@@ -278,3 +278,22 @@ def test_launch_shapes_and_schedules(ddg, block, min_blocks, schedule, cheap_lim
         assert (nodes == g["nodes_jpd5"]).all()
     finally:
         s.close()
+
+
+@pytest.mark.parametrize("block,min_blocks", [(512, 1), (256, 2)])
+def test_flat_lead_moves(ddg, block, min_blocks):
+    """The lead-move phase with its (lane, candidate) pairs spread over the block orders the
+    moves as the per-lane loop does: the reference's tricks and node counts, job for job."""
+    s = ddg.Solver(tt_log2=10, jobs_per_deal=5, lanes=4096, block=block, min_blocks=min_blocks, flat_moves=1)
+    try:
+        for name in ("k8_120.npz", "k6_4096.npz"):
+            g = load_golden(name)
+            t, nodes, _ = device_solve(ddg, s, g["hands"])
+            assert (t == g["tricks"]).all() and (nodes == g["nodes_jpd5"]).all(), name
+        g = load_golden("k13_24.npz")
+        hands = np.ascontiguousarray(g["hands"][LIGHT_13])
+        t, nodes, _ = device_solve(ddg, s, hands)
+        assert (t == g["tricks"][LIGHT_13]).all()
+        assert (nodes == g["nodes_jpd5"].reshape(-1, 5)[LIGHT_13].reshape(-1)).all()
+    finally:
+        s.close()
