@@ -75,7 +75,8 @@ def parse(argv=None):
     p.add_argument("--block", type=int, default=0, help="threads (lanes) per block; 0 = library default (512)")
     p.add_argument("--min-blocks", type=int, default=0)
     p.add_argument("--schedule", type=int, default=0, help="0 block-phase kernel, 1 queue kernel")
-    p.add_argument("--flat-moves", type=int, default=0, help="1: lead-move weights spread over the block")
+    p.add_argument("--flat-moves", type=int, default=0,
+                   help="0 (default) / 1: lead-move weights spread over the block; -1: per-lane loop")
     p.add_argument("--set-size", type=int, default=SET_SIZE)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")

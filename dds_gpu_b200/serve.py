@@ -126,13 +126,14 @@ def main(argv=None):
     p.add_argument("--capacity", type=float, default=0.0, help="deals/s at full load (0 = measure it)")
     p.add_argument("--sample-every", type=int, default=50)
     p.add_argument("--modes", default="plain,guided", help="plain and/or guided (the learned guide in the stream)")
+    p.add_argument("--free-below", type=int, default=0, help="the solver's free_below (0 = its default)")
     p.add_argument("--out", default="")
     a = p.parse_args(argv)
     from . import Guide
     from .guide import load_weights
     # Both modes run on the same lanes: a guided stream leaves two SMs to the guide's kernels.
     sms = torch.cuda.get_device_properties(0).multi_processor_count
-    solver = Solver(tt_log2=10, jobs_per_deal=5, lanes=(sms - 2) * 512)
+    solver = Solver(tt_log2=10, jobs_per_deal=5, lanes=(sms - 2) * 512, free_below=a.free_below)
     guide = None
     try:
         cap = a.capacity

@@ -69,10 +69,11 @@ typedef struct ddg_config {
                            (all lanes on parts of one job share what they learn; 40 hard
                            deals per lead: 129 s against 191 s without helping); -1 = in
                            its own TT (240+ s) */
-  int flat_moves;       /* block-phase kernel: 1 = the lead-move phase computes the DDS
+  int flat_moves;       /* block-phase kernel: 0 or 1 = the lead-move phase computes the DDS
                            weights of all its (lane, candidate) pairs side by side over the
-                           block's threads, 0 = each lane's thread loops over its candidates;
-                           same move order and node counts either way */
+                           block's threads (13-card deals: 696 against 663 M nodes/s); -1 =
+                           each lane's thread loops over its candidates; same move order and
+                           node counts either way */
 } ddg_config;
 
 /* Counters of one solve call (device-side counters, summed over lanes). */

@@ -280,11 +280,12 @@ def test_launch_shapes_and_schedules(ddg, block, min_blocks, schedule, cheap_lim
         s.close()
 
 
-@pytest.mark.parametrize("block,min_blocks", [(512, 1), (256, 2)])
-def test_flat_lead_moves(ddg, block, min_blocks):
-    """The lead-move phase with its (lane, candidate) pairs spread over the block orders the
-    moves as the per-lane loop does: the reference's tricks and node counts, job for job."""
-    s = ddg.Solver(tt_log2=10, jobs_per_deal=5, lanes=4096, block=block, min_blocks=min_blocks, flat_moves=1)
+@pytest.mark.parametrize("block,min_blocks,flat", [(512, 1, 1), (256, 2, 1), (512, 1, -1)])
+def test_flat_lead_moves(ddg, block, min_blocks, flat):
+    """The lead-move phase with its (lane, candidate) pairs spread over the block (the
+    default) orders the moves as the per-lane loop (flat_moves = -1) does: both give the
+    reference's tricks and node counts, job for job."""
+    s = ddg.Solver(tt_log2=10, jobs_per_deal=5, lanes=4096, block=block, min_blocks=min_blocks, flat_moves=flat)
     try:
         for name in ("k8_120.npz", "k6_4096.npz"):
             g = load_golden(name)
