@@ -442,6 +442,19 @@ __device__ __forceinline__ void run_phase(BlockShared<BLOCK>& sh, long long base
   __syncthreads();
 }
 
+// Stage class of a lane in a free-running round: 0 the cheap stages (returns, next moves,
+// job starts, waits), 1 ENTER at a trick start, 2 ENTER inside a trick, 3 lead moves, 4
+// follow moves; -1 idle.
+__device__ __forceinline__ int free_class(const Lane& L) {
+  switch (L.stage) {
+    case ST_ENTER: return L.p.nplayed == 0 ? 1 : 2;
+    case ST_MOVES_LEAD: return 3;
+    case ST_MOVES_FOLLOW: return 4;
+    case ST_IDLE: return -1;
+    default: return 0;
+  }
+}
+
 // The lead-move phase with its work flattened: every (lane, candidate) pair of the phase
 // is one item, and the items are spread over all threads of the block, so the DDS lead
 // weights of one lane's candidates are computed side by side instead of in a loop whose
@@ -644,17 +657,48 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(BatchArgs a) {
           if (item < 0 && pos < total + c) item = w * 32 + select_bit(mw, pos - total);
           total += c;
         }
+      // Each warp then steps its lanes, one stage at a time, choosing each time the stage
+      // class that most of its lanes are in (the warp-synchronous stage machine of the
+      // reference's wave_kernel, gpu/gpu_main.cu:61-152, per warp): the lanes of one step
+      // run one code region together instead of each thread walking its own lane through
+      // every stage, which would scatter a warp over the whole kernel's code. A lane that
+      // can make no progress (waiting for a job, a task or a helper) sits out the round.
+      DevEnv env;
+      bool parked = true, may_claim = false;
       if (item >= 0) {
         Lane& L = sh.lane[item];
         if (L.stage == ST_HUNGRY && sh.all_done) {
           atomicAdd(&a.tasks->hungry, -1);
           L.stage = ST_IDLE;
         } else if (L.stage != ST_IDLE) {
-          DevEnv env = lane_env(sh, base + item, item);
+          env = lane_env(sh, base + item, item);
           if (env.tp && task_abandoned(L, env.tp)) abort_task(L, env);
-          const bool may_claim = L.stage == ST_HUNGRY && atomicSub(&sh.claim_slots, 1) > 0;
-          advance_free(L, env, a.free_steps, may_claim);
+          may_claim = L.stage == ST_HUNGRY && atomicSub(&sh.claim_slots, 1) > 0;
+          parked = false;
         }
+      }
+      for (int k = 0; k < a.free_steps; k++) {
+        const int cls = parked ? -1 : free_class(sh.lane[item]);
+        int best = -1, best_n = 0;
+#pragma unroll
+        for (int c = 0; c < 5; c++) {
+          const int cnt = __popc(__ballot_sync(0xFFFFFFFFu, cls == c));
+          if (cnt > best_n) {
+            best_n = cnt;
+            best = c;
+          }
+        }
+        if (best < 0) break;  // every lane of the warp is idle or waiting
+        if (cls == best) {
+          Lane& L = sh.lane[item];
+          const int before = L.stage;
+          advance_free(L, env, 1, may_claim && before == ST_HUNGRY);
+          if (before == ST_HUNGRY && L.stage != ST_HUNGRY) may_claim = false;
+          if (L.stage == ST_IDLE ||
+              ((before == ST_TAKE || before == ST_HUNGRY || before == ST_WAIT) && L.stage == before))
+            parked = true;
+        }
+        __syncwarp();
       }
       __syncthreads();
       if (tid == 0) {
@@ -901,7 +945,10 @@ __device__ __forceinline__ void block_counters(BlockShared<BLOCK>& sh, const Bat
         case CNT_BOUNDS: sum += c.s.bounds; break;
         case CNT_ENTRY_READS: sum += c.s.tt.entry_reads; break;
         default:
+#ifdef DDG_EXIT_COUNTS
           if (tid >= CNT_EXIT && tid < CNT_EXIT + 7) sum += c.s.enter_exit[tid - CNT_EXIT];
+#endif
+          break;
       }
     }
     if (tid >= CNT_PHASE_WARPS && tid < CNT_PHASE_WARPS + PH_COUNT) sum = sh.ph_warps[tid - CNT_PHASE_WARPS];

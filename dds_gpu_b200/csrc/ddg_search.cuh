@@ -86,12 +86,26 @@ DDG_HD void frame_store(Frame* p, const Frame& f) {
 }
 
 // Search counters of one lane (per launch).
+// ENTER outcome counts (trivial, last trick, TT hit, quick tricks, later tricks, QT 2nd
+// hand, expanded) are diagnostics: kept in the bounds-checked build and the host replay
+// (DDG_EXIT_COUNTS), left out of the production kernel, whose per-lane counters live in
+// shared memory, where every byte taken from the L1 data cache is felt.
+#ifdef DDG_BOUNDS_CHECK
+#define DDG_EXIT_COUNTS 1
+#endif
 struct LaneStats {
   u64 nodes;
   TTStats tt;
-  u32 enter_exit[7];  // trivial, last trick, TT hit, quick tricks, later tricks, QT 2nd hand, expanded
+#ifdef DDG_EXIT_COUNTS
+  u32 enter_exit[7];
+#endif
   u32 bounds;         // bounds-checked builds: accesses out of range, skipped
 };
+#ifdef DDG_EXIT_COUNTS
+#define DDG_EXIT(st, k) ((st).enter_exit[k]++)
+#else
+#define DDG_EXIT(st, k) ((void)0)
+#endif
 
 // Frames per lane: the root and at most 52 plies below it, plus one spare (the reference's
 // dd_search keeps 53 frames, src/dd.h:802).
@@ -223,11 +237,11 @@ DDG_CALL int enter_lead(Pos& p, int target, Frame& f, u64& rel, Top& top, TTBuck
   st.nodes++;
   rel = 0;
   if (p.ns_won >= target) {
-    st.enter_exit[0]++;
+    DDG_EXIT(st, 0);
     return 1;
   }
   if (p.ns_won + p.left < target) {
-    st.enter_exit[0]++;
+    DDG_EXIT(st, 0);
     return 0;
   }
   const int need = target - p.ns_won;
@@ -238,7 +252,7 @@ DDG_CALL int enter_lead(Pos& p, int target, Frame& f, u64& rel, Top& top, TTBuck
     u64 in = all & suit_cards(s);
     int hi = top_bit(in);
     if (popc(in) >= 2) rel = card_bit(hi);
-    st.enter_exit[1]++;
+    DDG_EXIT(st, 1);
     return ns_side(holder_of(p.h, hi)) ? 1 : 0;
   }
   Hands hs;
@@ -248,7 +262,7 @@ DDG_CALL int enter_lead(Pos& p, int target, Frame& f, u64& rel, Top& top, TTBuck
   const ProbeOut pr = tt_probe(tt, key, need, st.tt);
   if (pr.hit >= 0) {
     rel = pr.rel;
-    st.enter_exit[2]++;
+    DDG_EXIT(st, 2);
     return pr.hit;
   }
   top = make_top(hs, key.lens);
@@ -260,13 +274,13 @@ DDG_CALL int enter_lead(Pos& p, int target, Frame& f, u64& rel, Top& top, TTBuck
   if (qo.decided) {
     val = ns_lead ? qo.q != 0 : qo.q == 0;
     wr = qo.wr;
-    st.enter_exit[3]++;
+    DDG_EXIT(st, 3);
   } else {
     const BoundOut lt = later_tricks(top, p.trump, p.leader, p.ns_won, p.left, target);
     if (lt.v) {
       val = !ns_lead;
       wr = lt.wr;
-      st.enter_exit[4]++;
+      DDG_EXIT(st, 4);
     }
   }
   if (val >= 0) {  // one store for both bounds, so lanes that decided either way store together
@@ -275,7 +289,7 @@ DDG_CALL int enter_lead(Pos& p, int target, Frame& f, u64& rel, Top& top, TTBuck
     return val;
   }
   open_frame(f, p.leader, need, p.left, pr.hint);
-  st.enter_exit[6]++;
+  DDG_EXIT(st, 6);
   return -1;
 }
 
@@ -295,12 +309,12 @@ DDG_CALL int enter_follow(Pos& p, int target, Frame& f, u64& rel, LaneStats& st)
     const BoundOut q2 = quick_tricks_2nd(hs, top, p.trump, second, trick_at(p, 0), cutoff);
     if (q2.v) {
       rel = q2.wr;
-      st.enter_exit[5]++;
+      DDG_EXIT(st, 5);
       return ns_side(second) ? 1 : 0;
     }
   }
   open_frame(f, (p.leader + p.nplayed) & 3, 0, 0, -1);
-  st.enter_exit[6]++;
+  DDG_EXIT(st, 6);
   return -1;
 }
 

@@ -84,7 +84,9 @@ typedef struct ddg_stats {
   uint64_t tt_stores;      /* TT stores that reached the bucket */
   uint64_t tt_bytes;       /* TT bytes read + written (tag lines, entries) */
   uint64_t enter_exit[7];  /* ENTER outcomes: trivial, last trick, TT hit, quick tricks,
-                              later tricks, 2nd-hand quick tricks, expanded */
+                              later tricks, 2nd-hand quick tricks, expanded; counted by
+                              libddg_check.so only (zero in libddg.so, whose per-lane
+                              counters are kept small to leave shared memory to L1) */
   uint64_t phase_warps[5]; /* warp passes per phase of the block loop: cheap stages, ENTER at
                               a trick start, ENTER inside a trick, lead moves, follow moves */
   uint64_t phase_items[5]; /* lanes served by those passes; items / (32 * warps) is the

@@ -10,6 +10,7 @@
 #include <thread>
 #include <vector>
 
+#define DDG_EXIT_COUNTS 1  // the replay reports the ENTER outcomes
 #include "ddg_search.cuh"
 
 using namespace ddg;
