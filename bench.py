@@ -33,7 +33,10 @@ bandwidth. cpu_baseline / --impl reference: the reference's own CPU solver
 (dd_solve_strain from its src/dd.h, compiled into oracle/_ref/cpu_window, which also makes
 the deals itself) on every host core over the same slices. parity: every job of deals
 [0, 2,000) that a run finished against the reference's tables, and every job the GPU and
-the CPU run both finished against each other.
+the CPU run both finished against each other. same_deals (N = 1): the reference's own GPU
+solver (its wave_kernel, gpu/gpu_main.cu built for sm_100a into oracle/_ref/dd_gpu_ref, in
+the reference arm's line) and this solver (its dd_gpu, in this arm's line) each run a
+--wave-s window on one Pgx file of deals [0, 2,000), checked against its tables.
 """
 import argparse
 import json
@@ -81,6 +84,8 @@ def parse(argv=None):
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-guide", action="store_true", help="plain solver only (no learned guide)")
+    p.add_argument("--wave-s", type=float, default=10.0,
+                   help="seconds per run of the same-deals comparison with the reference's GPU solver (0 = skip)")
     p.add_argument("--profile-case", action="store_true",
                    help="warm-up slices then one slice, nothing else (the launch to capture under ncu)")
     return p.parse_args(argv)
@@ -188,6 +193,47 @@ def cpu_measure(a, costs, size=BENCH_SET):
             "job_ms": {"p50": r["job_ms_p50"], "p99": r["job_ms_p99"]}}, tables
 
 
+def run_dd_gpu(exe, path, n, env, timeout=300):
+    """One `dd_gpu FILE.npy 0 n 10` run (the reference's gpu/gpu_main.cu driver or this
+    project's, same argv and output lines): every finished result is checked against the
+    file's tables; returns rc, wrong/checked, finished jobs and the node rate."""
+    import re
+    r = subprocess.run([exe, path, "0", str(n), "10"], capture_output=True, text=True, timeout=timeout,
+                       env=dict(os.environ, **env))
+    out = r.stdout
+    m = re.search(r"^GPU: ([0-9.]+)s, [0-9]+ deals/s \([0-9]+ strain-solves/s\), ([0-9]+) nodes/solve$", out, re.M)
+    w = re.search(r"^([0-9]+) wrong of ([0-9]+) checked$", out, re.M)
+    f = re.search(r"^finished jobs: ([0-9]+) in", out, re.M)
+    if not (m and w and f):
+        return {"rc": r.returncode, "error": (out + r.stderr)[-400:]}
+    sec, nodes_per_solve = float(m.group(1)), float(m.group(2))
+    return {"rc": r.returncode, "wrong": int(w.group(1)), "checked": int(w.group(2)), "jobs": int(f.group(1)),
+            "seconds": sec, "nodes_per_s": nodes_per_solve * n * JPD / sec}
+
+
+def same_deals(a, exe, runs):
+    """The reference's GPU solver (`wave_kernel`) and this one on one Pgx file: deals
+    [0, 2,000) of the benchmark set with the reference CPU solver's tables, a.wave_s
+    seconds each (TIME_LIMIT). `runs` maps a name to the driver's environment."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import pgx_np
+    if not (os.path.exists(exe) and os.path.exists(SAMPLE)):
+        return {"unavailable": f"{os.path.relpath(exe, ROOT)} or the 2,000-deal fixture is missing"}
+    with np.load(SAMPLE) as z:
+        hands, tricks = z["hands"], z["tricks"]
+    out = {"deals": f"deals [0, {len(hands)}) of the benchmark set in the Pgx .npy layout, checked against "
+                    "the reference CPU solver's tables",
+           "tt_log2": 10, "window_s": a.wave_s}
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "bench2000.npy")
+        pgx_np.write(path, hands, tricks)
+        for name, env in runs.items():
+            out[name] = run_dd_gpu(exe, path, len(hands), dict(env, TIME_LIMIT=f"{a.wave_s:g}"),
+                                   timeout=a.wave_s + 240)
+    return out
+
+
 def config_dict(a, world):
     return {"workload": WORKLOAD,
             "deal_set": (f"seed {SET_SEED}, K={SET_K}; deals [0, {BENCH_SET}) are the benchmark set, the solve runs "
@@ -212,6 +258,9 @@ def reference_arm(a, rank, world):
             "parity": {"checked": n, "equal": eq, "against": "reference tables of deals [0, 2000) (fixture)"},
             "cpu_baseline": {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
             "e2e": {"value": cpu["value"], "unit": "deals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if a.wave_s > 0 and world == 1:
+        line["same_deals"] = same_deals(a, os.path.join(ROOT, "oracle", "_ref", "dd_gpu_ref"), {
+            "reference_wave_kernel_32768_threads": {"WAVE": "1", "THREADS": "32768", "CHECK": "0"}})
     print(json.dumps(line), flush=True)
 
 
@@ -517,8 +566,11 @@ def our_arm(a, rank, world, local_rank):
         line["cpu_baseline"].update({"nodes_per_s": cpu["nodes_per_s"],
                                      "finished_deals_per_s": cpu["finished_deals_per_s"], "job_ms": cpu["job_ms"]})
         line["vs_cpu_nodes_per_s"] = s_head["nodes_per_s"] / cpu["nodes_per_s"] if cpu["nodes_per_s"] else None
-    print(json.dumps(line), flush=True)
     solver.close()
+    if a.wave_s > 0 and world == 1:
+        exe = os.path.join(ROOT, "dds_gpu_b200", "_lib", "dd_gpu")
+        line["same_deals"] = same_deals(a, exe, {"32768_lanes": {"THREADS": "32768"}, "full_grid": {}})
+    print(json.dumps(line), flush=True)
 
 
 def main(argv=None):

@@ -333,6 +333,7 @@ static BatchArgs make_args(ddg_solver* s, const uint64_t* d_hands, int64_t n, co
   a.cheap_limit = s->cfg.cheap_limit == 0 ? 3 : s->cfg.cheap_limit < 0 ? 0 : s->cfg.cheap_limit;
   a.fuse_follow = s->cfg.schedule == 2;
   a.flat_moves = s->cfg.flat_moves >= 0;  // 0 = the default: flattened
+  a.free_pack = s->cfg.free_pack > 0 ? s->cfg.free_pack : 1;
   return a;
 }
 

@@ -85,6 +85,7 @@ struct BatchArgs {
   // BatchArgs has it off. `first_target` is the binary search's first target (0 = 7).
   int one_job, one_strain, one_decl, first_target;
   int flat_moves;        // the lead-move phase spreads (lane, candidate) pairs over the block
+  int free_pack;         // free-running rounds: busy lanes per warp (1 = one to a warp, spread)
 };
 
 // One finished deal of a stream: its sequence number and table; `flag` = record index + 1,
@@ -646,7 +647,19 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(BatchArgs a) {
         }
       }
       __syncthreads();
-      const int pos = (tid & 31) * (BLOCK / 32) + (tid >> 5);
+      // The busy lanes go to nw warps: ceil(busy / free_pack), at least as many as hold
+      // every waiting lane too, at most all of them (free_pack 1: one busy lane to a warp).
+      int nwork = 0, nall = 0;
+#pragma unroll
+      for (int w = 0; w < BLOCK / 32; w++) {
+        nwork += __popc(sh.mask[w]);
+        nall += __popc(sh.mask[w]) + __popc(sh.mask2[w]);
+      }
+      int nw = (nwork + a.free_pack - 1) / a.free_pack;
+      if (nw < (nall + 31) / 32) nw = (nall + 31) / 32;
+      if (nw > BLOCK / 32) nw = BLOCK / 32;
+      if (nw < 1) nw = 1;
+      const int pos = (tid >> 5) < nw ? (tid & 31) * nw + (tid >> 5) : BLOCK;
       int item = -1, total = 0;
 #pragma unroll
       for (int pass = 0; pass < 2; pass++)

@@ -74,6 +74,9 @@ typedef struct ddg_config {
                            block's threads (13-card deals: 696 against 663 M nodes/s); -1 =
                            each lane's thread loops over its candidates; same move order and
                            node counts either way */
+  int free_pack;        /* free-running rounds: the block's busy lanes are spread over
+                           ceil(busy / free_pack) warps (at least enough warps to hold them,
+                           at most all); 0 = 1, one lane to a warp */
 } ddg_config;
 
 /* Counters of one solve call (device-side counters, summed over lanes). */

@@ -23,7 +23,7 @@ def run_bench(*args, env=None):
 
 
 def test_reference_arm_line():
-    lines = run_bench("--impl", "reference", "--steps", "2", "--warmup", "2", "--slice-s", "1")
+    lines = run_bench("--impl", "reference", "--steps", "2", "--warmup", "2", "--slice-s", "1", "--wave-s", "0")
     assert len(lines) == 1
     d = json.loads(lines[0])
     assert KEYS <= set(d)
@@ -36,11 +36,12 @@ def test_reference_arm_line():
     # value = the CPU's node rate over the workload's mean nodes per deal
     assert abs(d["value"] - d["nodes_per_s"] / d["nodes_per_deal"]["nodes_per_deal"]) < 1e-9 * d["value"]
     assert d["parity"]["equal"] is True and d["parity"]["checked"] > 0
+    assert "same_deals" not in d  # the GPU comparison is skipped with --wave-s 0
 
 
 def test_reference_arm_loads_nothing_of_the_product():
     code = ("import sys, json; sys.argv = ['bench.py', '--impl', 'reference', '--steps', '1', '--warmup', '1', "
-            "'--slice-s', '0.5']; import bench; bench.main(sys.argv[1:]); "
+            "'--slice-s', '0.5', '--wave-s', '0']; import bench; bench.main(sys.argv[1:]); "
             "maps = open('/proc/self/maps').read(); print(json.dumps({'ddg': 'libddg' in maps}))")
     r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr[-2000:]

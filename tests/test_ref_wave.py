@@ -10,13 +10,12 @@ node rates are printed, not asserted: 10,000 jobs fill only part of either solve
 and in that regime the reference's kernel is the faster one (its 32,768 threads run a
 lane each over every SM; this solver's full-load phases are thinly filled)."""
 import os
-import re
-import subprocess
 
 import pytest
 
 from conftest import ROOT, load_golden
 import pgx_np
+import bench
 
 pytestmark = pytest.mark.gpu
 
@@ -25,16 +24,9 @@ OURS = os.path.join(ROOT, "dds_gpu_b200", "_lib", "dd_gpu")
 
 
 def run(exe, path, n, env):
-    r = subprocess.run([exe, path, "0", str(n), "10"], capture_output=True, text=True, timeout=300,
-                       env=dict(os.environ, **env))
-    out = r.stdout
-    m = re.search(r"^GPU: ([0-9.]+)s, [0-9]+ deals/s \([0-9]+ strain-solves/s\), ([0-9]+) nodes/solve$", out, re.M)
-    w = re.search(r"^([0-9]+) wrong of ([0-9]+) checked$", out, re.M)
-    f = re.search(r"^finished jobs: ([0-9]+) in", out, re.M)
-    assert m and w and f, out + r.stderr
-    sec, nodes_per_solve = float(m.group(1)), float(m.group(2))
-    return {"rc": r.returncode, "wrong": int(w.group(1)), "checked": int(w.group(2)), "jobs": int(f.group(1)),
-            "nodes_per_s": nodes_per_solve * n * 5 / sec}
+    r = bench.run_dd_gpu(exe, path, n, env)
+    assert "error" not in r, r
+    return r
 
 
 def test_same_deals_as_the_reference_wave_kernel(ddg, tmp_path, capsys):
