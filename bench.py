@@ -80,6 +80,8 @@ def parse(argv=None):
     p.add_argument("--schedule", type=int, default=0, help="0 block-phase kernel, 1 queue kernel")
     p.add_argument("--flat-moves", type=int, default=0,
                    help="0 (default) / 1: lead-move weights spread over the block; -1: per-lane loop")
+    p.add_argument("--free-below", type=int, default=0, help="the solver's free_below (0 = its default)")
+    p.add_argument("--free-pack", type=int, default=0, help="the solver's free_pack (0 = its default)")
     p.add_argument("--set-size", type=int, default=SET_SIZE)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
@@ -357,7 +359,8 @@ def our_arm(a, rank, world, local_rank):
     dev = torch.device("cuda", local_rank)
     deals = deal_set(rank, a.set_size)
     solver = ddg.Solver(tt_log2=a.tt_log2, lanes=a.lanes, block=a.block, jobs_per_deal=JPD, device=local_rank,
-                        min_blocks=a.min_blocks, schedule=a.schedule, flat_moves=a.flat_moves)
+                        min_blocks=a.min_blocks, schedule=a.schedule, flat_moves=a.flat_moves,
+                        free_below=a.free_below, free_pack=a.free_pack)
     n = deals.shape[0]
     host_in = torch.from_numpy(deals.view(np.int64)).pin_memory()
     dev_in = host_in.to(dev)
@@ -537,6 +540,7 @@ def our_arm(a, rank, world, local_rank):
                      if s_head["value"] is not None else "finished jobs / 5 / s (no node-cost sample)"),
         "tuning": {"lanes": stats[0]["lanes"] if stats else 0, "block": stats[0]["block"] if stats else a.block,
                    "schedule": a.schedule, "flat_moves": a.flat_moves,
+                   "free_below": a.free_below, "free_pack": a.free_pack,
                    "guide": ("learned guide: NS seeds (stepping search) + root leads" if head == "guided"
                              else "off (plain DDS move order)")},
         "nodes_per_s": s_head["nodes_per_s"], "nodes_per_deal": s_head["nodes_per_deal"],

@@ -192,6 +192,7 @@ int ddg_solver_create(const ddg_config* cfg_in, ddg_solver** out) {
   if (cfg.jobs_per_deal != 5 && cfg.jobs_per_deal != 20)
     return fail(DDG_E_ARG, "jobs_per_deal %d is not 5 or 20", cfg.jobs_per_deal);
   if (cfg.lanes < 0) return fail(DDG_E_ARG, "lanes %d < 0", cfg.lanes);
+  if (cfg.free_pack < 0 || cfg.free_pack > 32) return fail(DDG_E_ARG, "free_pack %d is not 0..32", cfg.free_pack);
   int ndev = 0;
   CUDA_TRY(cudaGetDeviceCount(&ndev));
   if (cfg.device < 0 || cfg.device >= ndev) return fail(DDG_E_ARG, "device %d of %d", cfg.device, ndev);
@@ -326,14 +327,14 @@ static BatchArgs make_args(ddg_solver* s, const uint64_t* d_hands, int64_t n, co
   a.share_tt = s->tasks && s->cfg.help_share_tt >= 0;  // 0 = the default: shared
   a.tt_users = s->tasks ? reinterpret_cast<int*>(reinterpret_cast<char*>(s->tasks) + (sizeof(TaskPool) + 255) / 256 * 256)
                         : nullptr;
-  a.free_below = s->cfg.free_below == 0 ? 64 : s->cfg.free_below < 0 ? 0 : s->cfg.free_below;
+  a.free_below = s->cfg.free_below == 0 ? 96 : s->cfg.free_below < 0 ? 0 : s->cfg.free_below;
   a.free_steps = s->cfg.free_steps > 0 ? s->cfg.free_steps : 256;
   a.next_job = s->counters + CNT_NEXT_JOB;
   a.spread = s->cfg.phase_spread;
   a.cheap_limit = s->cfg.cheap_limit == 0 ? 3 : s->cfg.cheap_limit < 0 ? 0 : s->cfg.cheap_limit;
   a.fuse_follow = s->cfg.schedule == 2;
   a.flat_moves = s->cfg.flat_moves >= 0;  // 0 = the default: flattened
-  a.free_pack = s->cfg.free_pack > 0 ? s->cfg.free_pack : 1;
+  a.free_pack = s->cfg.free_pack;  // 0: by the block's busy lanes
   return a;
 }
 

@@ -59,7 +59,7 @@ struct BatchArgs {
   TaskPool* tasks;       // helping: idle lanes take donated moves (tricks exact), or null
   int share_tt;          // helping: a helper searches in its donor's TT (else in its own)
   int* tt_users;         // helping with shared TTs: per lane, helpers searching in its TT
-  int free_below;        // fewer busy lanes than this in a block: each thread runs its own lane
+  int free_below;        // fewer busy lanes than this in a block: free-running rounds, no phases
   int free_steps;        // stages a lane runs per free-running round
   struct LaneSave* save; // resumable solve: lane states kept between launches, or null
   int resume;            // 1: lanes start from `save` (a later slice of the same solve)
@@ -85,7 +85,7 @@ struct BatchArgs {
   // BatchArgs has it off. `first_target` is the binary search's first target (0 = 7).
   int one_job, one_strain, one_decl, first_target;
   int flat_moves;        // the lead-move phase spreads (lane, candidate) pairs over the block
-  int free_pack;         // free-running rounds: busy lanes per warp (1 = one to a warp, spread)
+  int free_pack;         // free-running rounds: busy lanes per warp; 0 = 1 up to 8 busy lanes, else 32
 };
 
 // One finished deal of a stream: its sequence number and table; `flag` = record index + 1,
@@ -630,10 +630,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(BatchArgs a) {
     }
     if (busy_here < a.free_below) {
       // Few busy lanes: each lane runs on a thread of its own for a while, no phases. The
-      // lanes with search work go first, one to a warp (the k-th to warp k mod 16, the
-      // (k div 16)-th thread of it), so up to one lane per warp runs at a lone lane's speed
-      // instead of sharing a warp's issue with the divergent paths of its neighbours;
-      // lanes waiting for a job or a task come after them.
+      // lanes with search work go first, round-robin over the round's nw warps (the k-th
+      // to warp k mod nw, the (k div nw)-th thread of it); lanes waiting for a job or a
+      // task come after them.
       const long long f0 = clock64();
       {
         const int wid = tid >> 5, ln = tid & 31;
@@ -647,29 +646,34 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(BatchArgs a) {
         }
       }
       __syncthreads();
-      // The busy lanes go to nw warps: ceil(busy / free_pack), at least as many as hold
-      // every waiting lane too, at most all of them (free_pack 1: one busy lane to a warp).
-      int nwork = 0, nall = 0;
+      // The busy lanes go to the first nw warps, nw = ceil(busy / pack) (at most all of
+      // them), the waiting lanes to the other threads. Few warps share their instruction fetches
+      // (spread over all 16 warps, 68 busy lanes per block stalled 4.6 cycles per issue
+      // on instruction fetch and searched 74 M nodes/s over the GPU; packed 32 to a warp,
+      // 169 M); a handful of lanes runs faster one to a warp, on the SM's four
+      // schedulers (5 lanes per block: 38 against 34 M nodes/s). pack = free_pack, or
+      // by default 1 up to 8 busy lanes and 32 above.
+      int nwork = 0;
 #pragma unroll
-      for (int w = 0; w < BLOCK / 32; w++) {
-        nwork += __popc(sh.mask[w]);
-        nall += __popc(sh.mask[w]) + __popc(sh.mask2[w]);
-      }
-      int nw = (nwork + a.free_pack - 1) / a.free_pack;
-      if (nw < (nall + 31) / 32) nw = (nall + 31) / 32;
+      for (int w = 0; w < BLOCK / 32; w++) nwork += __popc(sh.mask[w]);
+      const int pack = a.free_pack > 0 && a.free_pack <= 32 ? a.free_pack : (nwork <= 8 ? 1 : 32);
+      int nw = (nwork + pack - 1) / pack;
       if (nw > BLOCK / 32) nw = BLOCK / 32;
       if (nw < 1) nw = 1;
-      const int pos = (tid >> 5) < nw ? (tid & 31) * nw + (tid >> 5) : BLOCK;
+      // Thread (warp w < nw, lane l) takes busy lane number l*nw + w when that is below
+      // nwork; the other threads, those of warps nw.. first, then the unused ones of the
+      // first nw warps, take the waiting lanes in order (BLOCK threads hold all BLOCK lanes).
+      const int wid_ = tid >> 5, p = (tid & 31) * nw + wid_;
+      const bool takes_work = wid_ < nw && p < nwork;
+      const int rank = takes_work ? p : wid_ >= nw ? tid - nw * 32 : (BLOCK - nw * 32) + (p - nwork);
       int item = -1, total = 0;
 #pragma unroll
-      for (int pass = 0; pass < 2; pass++)
-#pragma unroll
-        for (int w = 0; w < BLOCK / 32; w++) {
-          const unsigned mw = pass ? sh.mask2[w] : sh.mask[w];
-          const int c = __popc(mw);
-          if (item < 0 && pos < total + c) item = w * 32 + select_bit(mw, pos - total);
-          total += c;
-        }
+      for (int w = 0; w < BLOCK / 32; w++) {
+        const unsigned mw = takes_work ? sh.mask[w] : sh.mask2[w];
+        const int c = __popc(mw);
+        if (item < 0 && rank < total + c) item = w * 32 + select_bit(mw, rank - total);
+        total += c;
+      }
       // Each warp then steps its lanes, one stage at a time, choosing each time the stage
       // class that most of its lanes are in (the warp-synchronous stage machine of the
       // reference's wave_kernel, gpu/gpu_main.cu:61-152, per warp): the lanes of one step

@@ -83,9 +83,9 @@ extern "C" int ddg_solve_static(const uint64_t* d_hands, int64_t n, uint8_t* d_o
   a.stacks = reinterpret_cast<ddg::Frame*>(slot.base + OFF_STACKS);
   a.lane_gen = reinterpret_cast<ddg::u32*>(slot.base + OFF_GEN);
   a.tt_log2 = STATIC_TT_LOG2;
-  a.free_below = 64;
+  a.free_below = 96;
   a.free_steps = 256;
-  a.free_pack = 1;
+  a.free_pack = 0;
   a.cheap_limit = 3;  // the pooled solver's default schedule (ddg_config.cheap_limit = 0)
   CUDA_TRY(cudaMemsetAsync(a.counters, 0, CNT_BYTES, stream));
   CUDA_TRY(cudaMemsetAsync(d_out20, 0xFF, (size_t)n * 20, stream));

@@ -42,3 +42,11 @@ def test_no_cpu_fallback_without_device(ddg):
         pytest.skip("a device is present")
     with pytest.raises(ddg.DDGError):
         ddg.Solver(lanes=128)
+
+
+def test_config_checked_before_any_device_call(ddg):
+    """Out-of-range configuration is refused with its own message (no device needed)."""
+    with pytest.raises(ddg.DDGError, match="free_pack"):
+        ddg.Solver(free_pack=33)
+    with pytest.raises(ddg.DDGError, match="tt_log2"):
+        ddg.Solver(tt_log2=30)

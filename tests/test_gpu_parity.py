@@ -298,3 +298,25 @@ def test_flat_lead_moves(ddg, block, min_blocks, flat):
         assert (nodes == g["nodes_jpd5"].reshape(-1, 5)[LIGHT_13].reshape(-1)).all()
     finally:
         s.close()
+
+
+@pytest.mark.parametrize("free_pack", [1, 8, 32])
+def test_free_rounds_packing(ddg, free_pack):
+    """Blocks that run only free-running rounds (free_below above the block size), with
+    their busy lanes one to a warp (free_pack 1), eight to a warp, or packed into as few
+    warps as hold them (32): which warp steps a lane changes nothing in its search, so the
+    tricks and node counts are the reference's, job for job."""
+    s = ddg.Solver(tt_log2=10, jobs_per_deal=5, lanes=4096, free_below=1024, free_pack=free_pack)
+    try:
+        for name in ("k8_120.npz", "k6_4096.npz"):
+            g = load_golden(name)
+            t, nodes, _ = device_solve(ddg, s, g["hands"])
+            assert (t == g["tricks"]).all() and (nodes == g["nodes_jpd5"]).all(), name
+        g = load_golden("k13_24.npz")
+        hands = np.ascontiguousarray(g["hands"][LIGHT_13])
+        t, nodes, _ = device_solve(ddg, s, hands)
+        assert (t == g["tricks"][LIGHT_13]).all()
+        assert (nodes == g["nodes_jpd5"].reshape(-1, 5)[LIGHT_13].reshape(-1)).all()
+        assert s.last_stats["free_rounds"] > 0 and s.last_stats["phase_warps"] == [0] * 5
+    finally:
+        s.close()
