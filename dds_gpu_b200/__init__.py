@@ -38,7 +38,7 @@ class _Config(ctypes.Structure):
                 ("mem_fraction", ctypes.c_double), ("help", ctypes.c_int), ("free_below", ctypes.c_int),
                 ("free_steps", ctypes.c_int), ("phase_spread", ctypes.c_int),
                 ("cheap_limit", ctypes.c_int), ("help_share_tt", ctypes.c_int), ("flat_moves", ctypes.c_int),
-                ("free_pack", ctypes.c_int), ("free_flat", ctypes.c_int)]
+                ("free_pack", ctypes.c_int)]
 
 
 class _Stats(ctypes.Structure):
@@ -166,8 +166,7 @@ class Solver:
 
     def __init__(self, tt_log2=10, lanes=0, block=0, jobs_per_deal=5, device=0, schedule=0,
                  time_limit_s=0.0, mem_fraction=0.85, min_blocks=0, help=0, free_below=0, free_steps=0,
-                 phase_spread=0, cheap_limit=0, library=None, help_share_tt=0, flat_moves=0, free_pack=0,
-                 free_flat=0):
+                 phase_spread=0, cheap_limit=0, library=None, help_share_tt=0, flat_moves=0, free_pack=0):
         lib = library or load_library()
         cfg = _Config()
         lib.ddg_config_default(ctypes.byref(cfg))
@@ -181,7 +180,6 @@ class Solver:
         cfg.help_share_tt = help_share_tt
         cfg.flat_moves = flat_moves
         cfg.free_pack = free_pack
-        cfg.free_flat = free_flat
         cfg.time_limit_s, cfg.mem_fraction = time_limit_s, mem_fraction
         self._lib = lib
         self._h = P()

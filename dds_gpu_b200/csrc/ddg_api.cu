@@ -335,7 +335,6 @@ static BatchArgs make_args(ddg_solver* s, const uint64_t* d_hands, int64_t n, co
   a.fuse_follow = s->cfg.schedule == 2;
   a.flat_moves = s->cfg.flat_moves >= 0;  // 0 = the default: flattened
   a.free_pack = s->cfg.free_pack;  // 0: by the block's busy lanes
-  a.free_flat = s->cfg.free_flat > 0;
   return a;
 }
 

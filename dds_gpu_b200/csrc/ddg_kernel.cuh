@@ -86,7 +86,6 @@ struct BatchArgs {
   int one_job, one_strain, one_decl, first_target;
   int flat_moves;        // the lead-move phase spreads (lane, candidate) pairs over the block
   int free_pack;         // free-running rounds: busy lanes per warp; 0 = 1 up to 8 busy lanes, else 32
-  int free_flat;         // free-running rounds: a warp's lead-move weights spread over its threads
 };
 
 // One finished deal of a stream: its sequence number and table; `flag` = record index + 1,
@@ -555,75 +554,6 @@ __device__ __forceinline__ void run_moves_lead_flat(BlockShared<BLOCK>& sh, long
   __syncthreads();
 }
 
-// The same for one warp of a free-running round: `item` is the thread's lane when it is at
-// its lead moves (else -1); the warp's (lane, candidate) pairs are spread over its 32
-// threads, each warp using its own 32 slots of the flat-list scratch (no phase runs
-// during a free-running round). The lanes end at ST_NEXT, as step_moves leaves them.
-template <int BLOCK>
-__device__ __forceinline__ void warp_moves_lead_flat(BlockShared<BLOCK>& sh, int item, DevEnv& env, int wid, int ln) {
-  const int s0 = wid * 32;
-  int cnt = 0;
-  u64 cand = 0;
-  if (item >= 0) {
-    const Lane& L = sh.lane[item];
-    int hint = frame_hint(L.f);
-    if (hint < 0 && L.sp == 0 && L.task < 0) {
-      const int h = env.root_hint(L);
-      if (h >= 0 && h < 64 && (hand_at(L.p.h, L.p.leader) >> h & 1)) hint = h;
-    }
-    u64 all;
-    cand = candidates(L.p, L.p.leader, all);
-    cnt = popc(cand);
-    sh.fl_cand[s0 + ln] = cand;
-    sh.fl_all[s0 + ln] = all;
-    sh.fl_item[s0 + ln] = (uint16_t)item;
-    sh.fl_hint[s0 + ln] = (int8_t)hint;
-  }
-  int incl = cnt;
-#pragma unroll
-  for (int d = 1; d < 32; d <<= 1) {
-    const int v = __shfl_up_sync(0xFFFFFFFFu, incl, d);
-    if (ln >= d) incl += v;
-  }
-  const int work = __shfl_sync(0xFFFFFFFFu, incl, 31), off = incl - cnt;
-  // Every slot gets its start (a slot with no candidates starts where the next one
-  // does), so the last slot starting at or before w is the one that holds pair w.
-  sh.fl_off[s0 + ln] = (uint16_t)off;
-  __syncwarp();
-  int16_t* score_of = sh.fl_score + s0 * 13;
-  for (int w = ln; w < work; w += 32) {
-    int lo = 0, hi = 31;
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (sh.fl_off[s0 + mid] <= w) lo = mid;
-      else hi = mid - 1;
-    }
-    u64 rest = sh.fl_cand[s0 + lo];
-    for (int k = w - sh.fl_off[s0 + lo]; k > 0; k--) rest ^= card_bit(top_bit(rest));
-    const int card = top_bit(rest);
-    const Lane& L = sh.lane[sh.fl_item[s0 + lo]];
-    Hands hs;
-    for (int i = 0; i < 4; i++) hs.h[i] = L.p.h[i];
-    const int hint = sh.fl_hint[s0 + lo];
-    const bool hinted = hint >= 0 && alike(hand_at(L.p.h, L.p.leader), sh.fl_all[s0 + lo], hint, card);
-    score_of[w] = (int16_t)lead_weight(hs, L.top, L.p.trump, L.p.left, L.p.leader, card, hinted);
-  }
-  __syncwarp();
-  if (item >= 0) {
-    Lane& L = sh.lane[item];
-    int n = 0, score[13], card_of[13];
-    u64 rest = cand;
-    for (int k = 0; k < cnt; k++) {
-      const int card = top_bit(rest);
-      rest ^= card_bit(card);
-      insert_move(score, card_of, n, card, score_of[off + k]);
-    }
-    pack_moves(L.f, card_of, n);
-    L.stage = ST_NEXT;
-  }
-  __syncwarp();
-}
-
 template <int BLOCK>
 __device__ __forceinline__ void block_counters(BlockShared<BLOCK>& sh, const BatchArgs& a, int tid);
 
@@ -776,9 +706,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(BatchArgs a) {
           }
         }
         if (best < 0) break;  // every lane of the warp is idle or waiting
-        if (best == 3 && a.free_flat) {  // the warp's lead moves, weights spread over its threads
-          warp_moves_lead_flat<BLOCK>(sh, cls == 3 ? item : -1, env, tid >> 5, tid & 31);
-        } else if (cls == best) {
+        if (cls == best) {
           Lane& L = sh.lane[item];
           const int before = L.stage;
           advance_free(L, env, 1, may_claim && before == ST_HUNGRY);

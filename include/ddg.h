@@ -80,10 +80,6 @@ typedef struct ddg_config {
                            at most all); 0 = one lane to a warp up to 8 busy lanes, else 32
                            to a warp (13-card deals, 68 busy lanes per block: 169 M nodes/s
                            packed against 74 M one to a warp) */
-  int free_flat;        /* free-running rounds: 1 = a warp's lead-move weights are computed
-                           side by side over its 32 threads (as flat_moves does over the
-                           block in the phases); 0 = each lane's thread loops over its
-                           candidates; same move order and node counts either way */
 } ddg_config;
 
 /* Counters of one solve call (device-side counters, summed over lanes). */

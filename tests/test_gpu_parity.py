@@ -300,15 +300,13 @@ def test_flat_lead_moves(ddg, block, min_blocks, flat):
         s.close()
 
 
-@pytest.mark.parametrize("free_pack,free_flat", [(1, 0), (8, 0), (32, 0), (1, 1), (32, 1)])
-def test_free_rounds_packing(ddg, free_pack, free_flat):
+@pytest.mark.parametrize("free_pack", [1, 8, 32])
+def test_free_rounds_packing(ddg, free_pack):
     """Blocks that run only free-running rounds (free_below above the block size), with
     their busy lanes one to a warp (free_pack 1), eight to a warp, or packed into as few
-    warps as hold them (32), and the lead-move weights computed by each lane's thread or
-    spread over its warp (free_flat): which threads step a lane changes nothing in its
-    search, so the tricks and node counts are the reference's, job for job."""
-    s = ddg.Solver(tt_log2=10, jobs_per_deal=5, lanes=4096, free_below=1024, free_pack=free_pack,
-                   free_flat=free_flat)
+    warps as hold them (32): which warp steps a lane changes nothing in its search, so the
+    tricks and node counts are the reference's, job for job."""
+    s = ddg.Solver(tt_log2=10, jobs_per_deal=5, lanes=4096, free_below=1024, free_pack=free_pack)
     try:
         for name in ("k8_120.npz", "k6_4096.npz"):
             g = load_golden(name)
