@@ -1,4 +1,5 @@
-"""The C-ABI library loads and exports every function include/ddg.h declares."""
+"""The C-ABI library loads and exports every function include/ddg.h declares, and the
+Python binding's structs match the header's layout."""
 import ctypes
 import os
 import re
@@ -50,3 +51,26 @@ def test_config_checked_before_any_device_call(ddg):
         ddg.Solver(free_pack=33)
     with pytest.raises(ddg.DDGError, match="tt_log2"):
         ddg.Solver(tt_log2=30)
+
+
+def test_struct_layouts_match_the_header(ddg, tmp_path):
+    """The ctypes mirrors of ddg_config and ddg_stats have the C header's size and every
+    field at the header's offset (a C program built against include/ddg.h prints them)."""
+    import subprocess
+    structs = {"ddg_config": ddg._Config, "ddg_stats": ddg._Stats}
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "ddg.h"', "int main(void) {"]
+    for cname, py in structs.items():
+        lines.append(f'  printf("{cname} %zu\\n", sizeof({cname}));')
+        for name, _ in py._fields_:
+            lines.append(f'  printf("{cname}.{name} %zu\\n", offsetof({cname}, {name}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c99", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = dict(ln.split() for ln in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                    check=True).stdout.splitlines())
+    for cname, py in structs.items():
+        assert int(got[cname]) == ctypes.sizeof(py), cname
+        for name, _ in py._fields_:
+            assert int(got[f"{cname}.{name}"]) == getattr(py, name).offset, f"{cname}.{name}"
