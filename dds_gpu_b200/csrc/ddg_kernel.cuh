@@ -651,8 +651,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(BatchArgs a) {
       // (spread over all 16 warps, 68 busy lanes per block stalled 4.6 cycles per issue
       // on instruction fetch and searched 74 M nodes/s over the GPU; packed 32 to a warp,
       // 169 M); a handful of lanes runs faster one to a warp, on the SM's four
-      // schedulers (5 lanes per block: 38 against 34 M nodes/s). pack = free_pack, or
-      // by default 1 up to 8 busy lanes and 32 above.
+      // schedulers (5 busy lanes per block: 36.8 M against 32.2 M packed). pack =
+      // free_pack, or by default 1 up to 8 busy lanes and 32 above.
       int nwork = 0;
 #pragma unroll
       for (int w = 0; w < BLOCK / 32; w++) nwork += __popc(sh.mask[w]);
