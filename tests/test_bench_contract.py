@@ -67,3 +67,24 @@ def test_gpus_mismatch_is_refused():
     r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--gpus", "4"], cwd=ROOT,
                        capture_output=True, text=True, timeout=120, env=env)
     assert r.returncode == 2 and "--gpus 4" in r.stderr
+
+
+def test_dd_gpu_output_parsing(tmp_path):
+    """same_deals reads the reference's `dd_gpu` output lines (gpu/gpu_main.cu:277,307,340);
+    a stand-in printing them is parsed into the node rate, the check and the finished jobs,
+    and a run without them is reported as an error, not a number."""
+    fake = tmp_path / "dd_gpu"
+    fake.write_text("#!/bin/sh\n"
+                    "echo '10048 threads, 2000 deals, 10000 solves, TT 320 KB/solve, 3.29 GB total'\n"
+                    "echo 'finished jobs: 2873 in 10.1 s = 56.8 full-job deals/s'\n"
+                    "echo 'GPU: 10.11s, 198 deals/s (989 strain-solves/s), 117550 nodes/solve'\n"
+                    "echo '0 wrong of 14132 checked'\n")
+    fake.chmod(0o755)
+    r = bench.run_dd_gpu(str(fake), "unused.npy", 2000, {})
+    assert r["rc"] == 0 and r["wrong"] == 0 and r["checked"] == 14132 and r["jobs"] == 2873
+    assert abs(r["nodes_per_s"] - 117550 * 2000 * 5 / 10.11) < 1e-6 * r["nodes_per_s"]
+    broken = tmp_path / "broken"
+    broken.write_text("#!/bin/sh\necho 'no device'\nexit 1\n")
+    broken.chmod(0o755)
+    r = bench.run_dd_gpu(str(broken), "unused.npy", 2000, {})
+    assert r["rc"] == 1 and "error" in r and "nodes_per_s" not in r
