@@ -663,9 +663,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) batch_kernel(BatchArgs a) {
       // Thread (warp w < nw, lane l) takes busy lane number l*nw + w when that is below
       // nwork; the other threads, those of warps nw.. first, then the unused ones of the
       // first nw warps, take the waiting lanes in order (BLOCK threads hold all BLOCK lanes).
-      const int wid_ = tid >> 5, p = (tid & 31) * nw + wid_;
-      const bool takes_work = wid_ < nw && p < nwork;
-      const int rank = takes_work ? p : wid_ >= nw ? tid - nw * 32 : (BLOCK - nw * 32) + (p - nwork);
+      const int wid = tid >> 5, p = (tid & 31) * nw + wid;
+      const bool takes_work = wid < nw && p < nwork;
+      const int rank = takes_work ? p : wid >= nw ? tid - nw * 32 : (BLOCK - nw * 32) + (p - nwork);
       int item = -1, total = 0;
 #pragma unroll
       for (int w = 0; w < BLOCK / 32; w++) {
