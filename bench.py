@@ -200,8 +200,11 @@ def run_dd_gpu(exe, path, n, env, timeout=300):
     project's, same argv and output lines): every finished result is checked against the
     file's tables; returns rc, wrong/checked, finished jobs and the node rate."""
     import re
-    r = subprocess.run([exe, path, "0", str(n), "10"], capture_output=True, text=True, timeout=timeout,
-                       env=dict(os.environ, **env))
+    try:
+        r = subprocess.run([exe, path, "0", str(n), "10"], capture_output=True, text=True, timeout=timeout,
+                           env=dict(os.environ, **env))
+    except (OSError, subprocess.TimeoutExpired) as e:
+        return {"rc": None, "error": f"{type(e).__name__}: {e}"[-400:]}
     out = r.stdout
     m = re.search(r"^GPU: ([0-9.]+)s, [0-9]+ deals/s \([0-9]+ strain-solves/s\), ([0-9]+) nodes/solve$", out, re.M)
     w = re.search(r"^([0-9]+) wrong of ([0-9]+) checked$", out, re.M)

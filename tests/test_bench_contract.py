@@ -88,3 +88,8 @@ def test_dd_gpu_output_parsing(tmp_path):
     broken.chmod(0o755)
     r = bench.run_dd_gpu(str(broken), "unused.npy", 2000, {})
     assert r["rc"] == 1 and "error" in r and "nodes_per_s" not in r
+    slow = tmp_path / "slow"
+    slow.write_text("#!/bin/sh\nsleep 30\n")
+    slow.chmod(0o755)
+    r = bench.run_dd_gpu(str(slow), "unused.npy", 2000, {}, timeout=1)
+    assert r["rc"] is None and "TimeoutExpired" in r["error"]
