@@ -12,7 +12,8 @@ endings; --nodes-per-deal). The stream keeps a device ring of 65,536 deal slots 
 admits deals as slots and lanes free up; deals that arrive while others are on the GPU
 start as soon as a lane is free (continuous batching).
 
-For each rate: deals arrive for --seconds; solved rate, in-flight deals (sampled every
+For each rate: deals arrive for --seconds (after --prefill deals at t = 0, if given);
+solved rate, in-flight deals (sampled every
 second) and the latency of every deal from its arrival to its result on the host, with
 p50 / p99 / p99.9 over the deals that arrived in the second half of the window (after the
 start-up) and finished before the drain limit; deals still running then are counted, not
@@ -57,11 +58,18 @@ def capacity(solver, seconds, torch):
     return st["nodes"] / (st["kernel_ms"] * 1e-3)
 
 
-def run_rate(solver, rate, seconds, drain_s, sample_every, seed, guide=None):
+def arrival_times(rate, seconds, seed, prefill=0):
+    """Arrival times (s, sorted): `prefill` deals at t = 0 (a backlog that brings the
+    stream near its steady in-flight count sooner), then a Poisson process of `rate`
+    deals/s up to `seconds`."""
     rng = np.random.default_rng(seed)
     gaps = rng.exponential(1.0 / rate, int(rate * seconds * 1.5) + 100)
     arrivals = np.cumsum(gaps)
-    arrivals = arrivals[arrivals < seconds]
+    return np.concatenate([np.zeros(prefill), arrivals[arrivals < seconds]])
+
+
+def run_rate(solver, rate, seconds, drain_s, sample_every, seed, guide=None, prefill=0):
+    arrivals = arrival_times(rate, seconds, seed, prefill)
     n = len(arrivals)
     hands, ks = mix_deals(seed, n)
     done_at = np.full(n, np.nan)
@@ -94,7 +102,7 @@ def run_rate(solver, rate, seconds, drain_s, sample_every, seed, guide=None):
     finally:
         stats = st.close(drain=False)
     lat = done_at - arrivals
-    second_half = arrivals >= seconds / 2
+    second_half = arrivals >= seconds / 2  # never a prefilled deal (they arrive at 0)
     fin = second_half & np.isfinite(lat)
     q = (lambda p: float(np.quantile(lat[fin], p) * 1e3)) if fin.any() else (lambda p: None)
     in_window = np.isfinite(done_at) & (done_at <= seconds)
@@ -102,7 +110,7 @@ def run_rate(solver, rate, seconds, drain_s, sample_every, seed, guide=None):
     mid = [v for t, v in in_flight if t <= seconds / 2]
     end = [v for t, v in in_flight if t <= seconds]
     return {
-        "arrival_rate": rate, "arrived": int(n), "admitted": int(submitted),
+        "arrival_rate": rate, "prefill": int(prefill), "arrived": int(n), "admitted": int(submitted),
         "solved_in_window": int(in_window.sum()), "solved_rate_2nd_half": float(half.sum() / (seconds / 2)),
         "arrived_rate_2nd_half": float(second_half.sum() / (seconds / 2)),
         "in_flight_mid": mid[-1] if mid else None, "in_flight_end": end[-1] if end else None,
@@ -127,6 +135,9 @@ def main(argv=None):
     p.add_argument("--sample-every", type=int, default=50)
     p.add_argument("--modes", default="plain,guided", help="plain and/or guided (the learned guide in the stream)")
     p.add_argument("--free-below", type=int, default=0, help="the solver's free_below (0 = its default)")
+    p.add_argument("--prefill", type=int, default=0,
+                   help="deals of the mix submitted at t = 0 before the Poisson arrivals (a backlog that "
+                        "brings the stream near its steady state sooner; not in the latency figures)")
     p.add_argument("--out", default="")
     a = p.parse_args(argv)
     from . import Guide
@@ -154,7 +165,7 @@ def main(argv=None):
                 if mode == "guided" and guide is None:
                     continue
                 r = run_rate(solver, f * cap, a.seconds, a.drain, a.sample_every, MIX_SEED + 100 + i,
-                             guide if mode == "guided" else None)
+                             guide if mode == "guided" else None, a.prefill)
                 r["fraction"] = f
                 r["mode"] = mode
                 rep["rates"].append(r)

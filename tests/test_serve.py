@@ -49,6 +49,19 @@ def test_mix_is_seeded_and_shaped(ddg):
     assert all(bin(int(x[0])).count("1") == kk for x, kk in zip(h, k))
 
 
+def test_arrival_times(ddg):
+    """A backlog of `prefill` deals at t = 0, then Poisson arrivals at the asked rate, sorted
+    and inside the window; the same seed gives the same schedule."""
+    from dds_gpu_b200 import serve
+    a = serve.arrival_times(20.0, 300.0, seed=5, prefill=150)
+    assert (a[:150] == 0).all() and (a[150:] > 0).all() and (np.diff(a) >= 0).all() and a[-1] < 300.0
+    assert abs((len(a) - 150) / 300.0 - 20.0) < 20.0 * 0.06  # 6,000 expected: within ~5 sigma
+    gaps = np.diff(a[150:])
+    assert abs(gaps.mean() - 1 / 20.0) < 0.05 / 20.0 * 5 and abs(gaps.std() / gaps.mean() - 1) < 0.1
+    assert (serve.arrival_times(20.0, 300.0, seed=5, prefill=150) == a).all()
+    assert len(serve.arrival_times(20.0, 300.0, seed=5)) == len(a) - 150
+
+
 @pytest.mark.gpu
 def test_poisson_stream_matches_reference(ddg):
     from dds_gpu_b200 import serve
